@@ -1,0 +1,155 @@
+/*
+ * stfwi.h -- C ABI of the B200 elastic velocity-strain solver.
+ *
+ * One handle = one padded grid + one shot batch on one CUDA device.  The
+ * handle owns its device workspace (fields, C-PML memory strips, strain
+ * history, gradient accumulators) and the batch's geometry.  Large inputs and
+ * outputs are passed as plain pointers that may be host or device memory
+ * (copies use cudaMemcpyDefault, so host pointers cost a transfer).  Calls
+ * on one handle must come from one thread; every call is asynchronous on the
+ * given stream unless it says otherwise.  Errors are status codes; a call
+ * never aborts the process and never traps the GPU.  stfwi_last_error()
+ * gives the message of the last failing call.
+ *
+ * The entry points replace the reference's Python functions
+ * (paths relative to the reference project):
+ *   stfwi_set_model + stfwi_forward  fwi/forward.py:119-501 (forward_jax) and
+ *                                    :508-544 (build_forward_fn -> run_shot)
+ *   stfwi_get_records                the (vx, vz, ex, ez) receiver tuple of
+ *                                    forward_jax, fwi/forward.py:465-469
+ *   stfwi_misfit                     fwi/gradient.py:139-156 (_shot_residual_prep
+ *                                    and its jax.grad), fwi/loss.py:92-118
+ *   stfwi_gradient(STFWI_GRAD_SRC)   fwi/adjoint_jax_kernel.py:61-483 (adjoint_jax)
+ *   stfwi_gradient(STFWI_GRAD_EXACT) the 'ad' backend, fwi/gradient.py:106-132
+ *   stfwi_gradient(STFWI_GRAD_IMAGING) the 'adjoint' backend's imaging,
+ *                                    fwi/gradient.py:159-259, fwi/imaging.py:83-169
+ *   stfwi_illumination               fwi/illumination.py:18-48 (Ws before cropping)
+ */
+#ifndef STFWI_H
+#define STFWI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    STFWI_OK = 0,
+    STFWI_ERR_INVALID = 1,     /* bad argument or descriptor (ValueError in the reference) */
+    STFWI_ERR_UNSUPPORTED = 2, /* fd_order / src_type not supported (NotImplementedError) */
+    STFWI_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    STFWI_ERR_OOM = 4,         /* workspace does not fit the memory budget */
+    STFWI_ERR_NONFINITE = 5,   /* a receiver sample became NaN/Inf (unstable model or dt) */
+    STFWI_ERR_STATE = 6        /* call order: e.g. gradient before a storing forward */
+} stfwi_status;
+
+typedef struct stfwi_handle stfwi_handle;
+
+/* Grid, time and batch description (the static arguments of forward_jax). */
+typedef struct {
+    int32_t nz_dom, nx_dom; /* physical model size (rows z, columns x) */
+    int32_t pad;            /* C-PML thickness in cells */
+    int32_t fd_order;       /* 2, 4 or 8 */
+    int32_t free_surface;   /* 1: free surface on top, PML on 3 sides */
+    int32_t nt;             /* time steps */
+    int32_t nrec;           /* receivers (shared by all shots) */
+    int32_t max_shots;      /* shot batch capacity */
+    double dx, dz, dt;      /* grid spacing [m], time step [s] */
+    double fc;              /* source peak frequency, used by the PML profile */
+    int32_t want_gradient;  /* 1: reserve strain history + accumulators */
+    int32_t shot_group;     /* shots per block (0: automatic) */
+    double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
+} stfwi_desc;
+
+/* source types */
+#define STFWI_SRC_FORCE 0  /* vertical force into Vz (fwi/forward.py:366-367) */
+#define STFWI_SRC_MOMENT 1 /* explosive moment into exx, ezz (fwi/forward.py:406-411) */
+
+/* stfwi_forward flags */
+#define STFWI_FWD_STORE 1u  /* keep the strain history a later stfwi_gradient needs */
+
+/* stfwi_gradient modes (bit set) */
+#define STFWI_GRAD_EXACT 1u   /* exact discrete gradient of the FP32 forward */
+#define STFWI_GRAD_IMAGING 2u /* the reference's continuous imaging formula */
+#define STFWI_GRAD_SRC 4u     /* source-wavelet adjoint (dot-product test) */
+
+/* Residual preparation: misfit_k = scale/nshot * mean_{t,r}(F T (pred - obs))^2
+ * on one receiver component; F = cascade of nsos biquads (b0 b1 b2 a0 a1 a2,
+ * scipy 'sos' layout, normalised by a0), T = cosine end taper of n_taper
+ * samples (fwi/filters.py). */
+typedef struct {
+    int32_t component; /* 0 vx, 1 vz, 2 exx, 3 ezz */
+    int32_t n_taper;
+    int32_t nsos;      /* 0: no filter; at most 16 sections */
+    int32_t reserved;
+    double scale;
+    const double *sos; /* host pointer, [nsos][6] */
+} stfwi_misfit_desc;
+
+size_t stfwi_workspace_bytes(const stfwi_desc *d);
+stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out);
+void stfwi_destroy(stfwi_handle *h);
+const char *stfwi_last_error(const stfwi_handle *h);
+
+/* Model (nz_dom x nx_dom float32 each, z-major): builds the padded-grid
+ * materials and C-PML profiles on the device. */
+stfwi_status stfwi_set_model(stfwi_handle *h, const float *vs, const float *vp, const float *rho,
+                             void *stream);
+
+/* Receivers in physical-domain indices (host arrays of nrec). */
+stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *rec_x,
+                                 const int32_t *rec_z);
+
+/* Shots: src = host [nshot][3] (x, z, type) in physical-domain indices;
+ * wavelets = [nshot][nt] float32 (host or device). */
+stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
+                             const float *wavelets, void *stream);
+
+/* Forward modelling of every shot of the batch in one launch per phase. */
+stfwi_status stfwi_forward(stfwi_handle *h, uint32_t flags, void *stream);
+
+/* Receiver traces of the last forward: [nshot][4][nt][nrec] (vx, vz, exx, ezz). */
+stfwi_status stfwi_get_records(stfwi_handle *h, float *out, void *stream);
+
+/* Misfit and adjoint sources from the last forward's traces.  obs =
+ * [nshot][nt][nrec] float32 (host or device); misfit_out = [nshot] FP64
+ * (host or device), per-shot terms whose sum is the reference's loss. */
+stfwi_status stfwi_misfit(stfwi_handle *h, const float *obs, const stfwi_misfit_desc *m,
+                          double *misfit_out, void *stream);
+
+/* Explicit adjoint sources [nshot][4][nt][nrec] (replaces stfwi_misfit's). */
+stfwi_status stfwi_set_adjoint_sources(stfwi_handle *h, const float *rec_adj, void *stream);
+
+/* Adjoint sweep.  mode: STFWI_GRAD_* bits.  g_out: for each of EXACT then
+ * IMAGING that is set, [3][nz_dom][nx_dom] FP64 = (dJ/dVs, dJ/dVp, dJ/drho)
+ * summed over shots (dJ/drho is only filled by IMAGING's Lame part; EXACT
+ * returns it as 0).  src_wav_a: [nshot][nt] float32 when SRC is set. */
+stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float *src_wav_a,
+                            void *stream);
+
+/* Source illumination Ws = Sum_shots Sum_t field^2 of one component on the
+ * padded grid, [nz_t][nx_t] FP64 (runs its own forward). */
+stfwi_status stfwi_illumination(stfwi_handle *h, int32_t component, double *ws_out, void *stream);
+
+/* Synchronises the stream and returns the device status word (0 = fine). */
+stfwi_status stfwi_check(stfwi_handle *h, void *stream);
+
+/* Sampled per-kernel timing (tracing).  With every > 0 the captured time
+ * loops record a CUDA event pair around each kernel of every `every`-th
+ * step; every = 0 turns it off.  Re-captures the graphs. */
+stfwi_status stfwi_profile(stfwi_handle *h, int32_t every);
+
+/* Sampled launch times of the passes run since the last call, as [4][2] =
+ * (total ms, launches) for the kernels fwd_vel, fwd_str, adj_a, adj_b.
+ * Synchronises the handle's stream; resets the sums. */
+stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out);
+
+/* Padded-grid shape of a descriptor. */
+void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

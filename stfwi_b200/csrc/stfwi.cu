@@ -1,0 +1,944 @@
+// C ABI of the B200 elastic velocity-strain solver: handle, workspace plan,
+// model/geometry set-up kernels, launch sequences (captured into CUDA graphs)
+// and the residual/misfit kernel.  Declarations: include/stfwi.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/stfwi.h"
+#include "kernels.cuh"
+
+using namespace stfwi;
+
+namespace {
+
+constexpr int MAX_SOS = 16;
+
+struct GraphKey {
+    int kind;    // 0 forward, 1 adjoint, 2 illumination
+    uint32_t flags;
+    int nshot;
+    bool operator<(const GraphKey &o) const
+    {
+        if (kind != o.kind) return kind < o.kind;
+        if (flags != o.flags) return flags < o.flags;
+        return nshot < o.nshot;
+    }
+};
+
+}  // namespace
+
+struct stfwi_handle {
+    stfwi_desc d{};
+    Geo g{};
+    int device = 0;
+    int groups = 1, spg = 1;  // shot groups per launch, shots per group
+    std::string err;
+
+    // model
+    float *vs = nullptr, *vp = nullptr, *rho = nullptr;     // physical [nd]
+    float *B = nullptr, *L2M = nullptr, *L = nullptr, *M = nullptr, *Lr = nullptr;
+    float *bx = nullptr, *ax = nullptr, *ikx = nullptr, *bz = nullptr, *az = nullptr, *ikz = nullptr;
+    float *vpmax = nullptr;
+    bool model_set = false;
+
+    // shots / receivers
+    int nshot = 0;
+    int *sx = nullptr, *sz = nullptr, *stype = nullptr;
+    float *wav = nullptr, *fcoef = nullptr, *mcoef = nullptr, *lm = nullptr;
+    int *tile_start = nullptr, *tile_rec = nullptr, *rx = nullptr, *rz = nullptr;
+    bool shots_set = false, recv_set = false;
+
+    // state
+    float *F = nullptr, *A = nullptr, *PX = nullptr, *PZ = nullptr;
+    float *rec = nullptr, *rec_adj = nullptr;
+    float *snap = nullptr, *row0 = nullptr;
+    int slots = 0;
+    double *acc = nullptr, *accLr = nullptr, *gtmp = nullptr;
+    double *energy = nullptr;
+    double *mis_trace = nullptr, *mis_shot = nullptr;
+    float *src_a = nullptr;
+    float *obs = nullptr;
+    int *status = nullptr;
+    bool stored = false;  // last forward kept its strain history
+
+    cudaStream_t hs = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // sampled kernel timing: pev[k] holds (start, stop) pairs per sampled step
+    int prof_every = 0;
+    std::vector<cudaEvent_t> pev[4];
+    double prof_ms[4] = {0, 0, 0, 0};
+    long long prof_cnt[4] = {0, 0, 0, 0};
+    std::map<GraphKey, cudaGraphExec_t> graphs;
+    size_t bytes = 0;
+};
+
+namespace {
+
+stfwi_status fail(stfwi_handle *h, stfwi_status st, const char *fmt, ...)
+{
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return st;
+}
+
+#define CK(h, call)                                                                         \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((h), STFWI_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                \
+    } while (0)
+
+struct Plan {
+    long long nz, nx, P, nd, zs_n, xs_n;
+    int tiles_x, tiles_z;
+    size_t fields, psi, snap, row0, acc, rec, misc;
+    size_t total() const { return fields + psi + snap + row0 + acc + rec + misc; }
+};
+
+int auto_groups(const stfwi_desc *d, int tiles)
+{
+    if (d->shot_group > 0) return std::max(1, (d->max_shots + d->shot_group - 1) / d->shot_group);
+    // enough blocks to fill 148 SMs a few times over, few enough that each
+    // block reuses its material tile and gradient registers across shots
+    int want = std::max(1, (4 * 148 + tiles - 1) / tiles);
+    return std::min(want, std::max(1, d->max_shots));
+}
+
+Plan make_plan(const stfwi_desc *d)
+{
+    Plan p{};
+    p.nx = d->nx_dom + 2LL * d->pad;
+    p.nz = d->free_surface ? d->nz_dom + (long long)d->pad : d->nz_dom + 2LL * d->pad;
+    p.P = (p.nx + 31) / 32 * 32;
+    p.nd = (long long)d->nz_dom * d->nx_dom;
+    p.xs_n = 2LL * d->pad;
+    p.zs_n = d->free_surface ? d->pad : 2LL * d->pad;
+    p.tiles_x = (int)((p.nx + TX - 1) / TX);
+    p.tiles_z = (int)((p.nz + TZ - 1) / TZ);
+    const long long S = d->max_shots;
+    const int G = auto_groups(d, p.tiles_x * p.tiles_z);
+    p.fields = (size_t)2 * S * F_N * p.nz * p.P * sizeof(float);
+    p.psi = (size_t)S * (NPX * p.nz * p.xs_n + NPZ * p.zs_n * p.P) * sizeof(float);
+    p.snap = d->want_gradient ? (size_t)S * d->nt * 3 * p.nd * sizeof(float) : 0;
+    p.row0 = (d->want_gradient && d->free_surface) ? (size_t)S * d->nt * d->nx_dom * sizeof(float) : 0;
+    p.acc = (size_t)G * (5 * p.nd + d->nx_dom) * sizeof(double) + 3 * p.nd * 2 * sizeof(double);
+    p.rec = (size_t)2 * S * 4 * d->nt * std::max(d->nrec, 1) * sizeof(float)
+          + (size_t)S * d->nt * std::max(d->nrec, 1) * sizeof(float);
+    p.misc = (size_t)(8 * p.nz * p.P + 4 * p.nd) * sizeof(float) + (size_t)p.nz * p.nx * sizeof(double)
+           + (size_t)S * (d->nt + 16) * sizeof(float) + (size_t)S * (std::max(d->nrec, 1) + 1) * sizeof(double)
+           + (1 << 20);
+    return p;
+}
+
+// ---------------------------------------------------------------- set-up kernels
+
+__global__ void k_materials(int nz, int nx, int P, int nz_dom, int nx_dom, int z0, int pad,
+                            const float *vs, const float *vp, const float *rho, float *B, float *L2M,
+                            float *L, float *M, float *Lr)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    if (j >= nx || i >= nz) return;
+    // nearest-neighbour extension into the PML (fwi/forward.py:195-212)
+    const int si = min(max(i - z0, 0), nz_dom - 1), sj = min(max(j - pad, 0), nx_dom - 1);
+    const long long s = (long long)si * nx_dom + sj;
+    const float r = rho[s], a = vs[s], b = vp[s];
+    // fwi/forward.py:222-231
+    const float m = r * (a * a), l2m = r * (b * b), l = l2m - 2.f * m;
+    const long long o = (long long)i * P + j;
+    B[o] = 1.0f / r;
+    L2M[o] = l2m;
+    L[o] = l;
+    M[o] = m;
+    if (i == 0) Lr[j] = -l / l2m;
+}
+
+__global__ void k_vpmax(const float *vp, long long n, float *out)
+{
+    __shared__ float red[1024];
+    float m = -INFINITY;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) m = fmaxf(m, vp[q]);
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// C-PML profiles (fwi/forward.py:35-104), as 1-D arrays: the reference's
+// 2-D coefficient arrays are constant along rows (x) / columns (z).
+__global__ void k_pml(int nz, int nx, int nz_dom, int pad, int fs, double dx, double dt, double fc,
+                      const float *vpmax, float *bx, float *ax, float *ikx, float *bz, float *az,
+                      float *ikz)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const double Lp = pad * dx;
+    // d0 with the float32 arithmetic of the reference's promotion rules
+    float d0f = -3.0f * vpmax[0];
+    d0f = d0f * (float)log(1e-3);
+    d0f = d0f / (float)(2.0 * Lp);
+    const double d0 = d0f;
+    auto coef = [&](int i, float *b, float *a, float *ik) {
+        if (i < 0) { *b = 1.f; *a = 0.f; *ik = 1.f; return; }
+        const double dist = (i + 1) * dx / Lp;
+        const double dd = d0 * (dist * dist), kk = 1.0 + (2.0 - 1.0) * (dist * dist);
+        const double al = M_PI * fc * (1.0 - dist);
+        const double bb = exp(-(dd / kk + al) * dt);
+        const double den = kk * (dd + kk * al);
+        *b = (float)bb;
+        *a = (float)(den > 1e-10 ? dd * (bb - 1.0) / den : 0.0);
+        *ik = (float)(1.0 / kk);
+    };
+    if (t < nx) {
+        int i = -1;
+        if (t < pad) i = pad - 1 - t;
+        else if (t >= nx - pad) i = t - (nx - pad);
+        coef(i, bx + t, ax + t, ikx + t);
+    }
+    if (t < nz) {
+        int i = -1;
+        const int bottom = fs ? nz_dom : pad + nz_dom;
+        if (t >= bottom) i = t - bottom;
+        else if (!fs && t < pad) i = pad - 1 - t;
+        coef(i, bz + t, az + t, ikz + t);
+    }
+}
+
+__global__ void k_src_coefs(int nshot, const int *sx, const int *sz, int P, const float *B,
+                            const float *L, const float *M, float dtdxdz, float dx, float dz,
+                            float *fcoef, float *mcoef, float *lm)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshot) return;
+    const long long o = (long long)sz[s] * P + sx[s];
+    fcoef[s] = dtdxdz * B[o];
+    const float lms = L[o] + M[o];
+    lm[s] = lms;
+    mcoef[s] = 2.f * lms * dx * dz;
+}
+
+// adjoint prologue: receiver injection of the last step into exx_a, ezz_a
+__global__ void k_inject_last(Geo g, const int *rx, const int *rz, const float *rec_adj, float *A)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nshot * g.nrec) return;
+    const int s = t / g.nrec, r = t % g.nrec;
+    const long long o = (long long)rz[r] * g.P + rx[r];
+    const float *src = rec_adj + (long long)s * 4 * g.nt * g.nrec + (long long)(g.nt - 1) * g.nrec + r;
+    atomicAdd(A + ((long long)s * F_N + F_EX) * g.fstride + o, src[2LL * g.nt * g.nrec]);
+    atomicAdd(A + ((long long)s * F_N + F_EZ) * g.fstride + o, src[3LL * g.nt * g.nrec]);
+}
+
+// Residual preparation (fwi/gradient.py:139-156, fwi/filters.py), one thread
+// per trace: r = F T (pred - obs); misfit = scale/nshot * mean(r^2);
+// cotangent = 2 scale/(nshot N) T^T F^T r, F^T being the time-reversed cascade.
+struct SosParams {
+    int nsos;
+    double c[MAX_SOS][5];  // b0 b1 b2 a1 a2, normalised by a0
+};
+
+__global__ void k_misfit(Geo g, int comp, int n_taper, SosParams sp, double scale, int nshot_norm,
+                         const float *rec, const float *obs, float *rec_adj, double *mis_trace)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nshot * g.nrec) return;
+    const int s = t / g.nrec, r = t % g.nrec;
+    const long long NR = g.nrec, NT = g.nt;
+    const float *pred = rec + (long long)s * 4 * NT * NR + comp * NT * NR + r;
+    const float *ob = obs + (long long)s * NT * NR + r;
+    float *out = rec_adj + (long long)s * 4 * NT * NR;
+    for (int c = 0; c < 4; ++c)
+        if (c != comp)
+            for (long long n = 0; n < NT; ++n) out[c * NT * NR + n * NR + r] = 0.f;
+    float *cot = out + comp * NT * NR + r;
+    const int tstart = g.nt - min(n_taper, g.nt);
+    const double npi = M_PI;
+    auto taper = [&](int n) -> double {
+        if (n_taper <= 0 || n < tstart) return 1.0;
+        const int m = n - tstart + 1;
+        return (cos((double)m / n_taper * npi) + 1.0) / 2.0;
+    };
+    double st[MAX_SOS][4];
+    for (int k = 0; k < sp.nsos; ++k) st[k][0] = st[k][1] = st[k][2] = st[k][3] = 0.0;
+    double sum = 0.0;
+    for (int n = 0; n < g.nt; ++n) {
+        const double tp = taper(n);
+        double x = tp * (double)pred[n * NR] - tp * (double)ob[n * NR];
+        for (int k = 0; k < sp.nsos; ++k) {
+            const double y = sp.c[k][0] * x + sp.c[k][1] * st[k][0] + sp.c[k][2] * st[k][1]
+                           - sp.c[k][3] * st[k][2] - sp.c[k][4] * st[k][3];
+            st[k][1] = st[k][0]; st[k][0] = x; st[k][3] = st[k][2]; st[k][2] = y;
+            x = y;
+        }
+        sum += x * x;
+        cot[n * NR] = (float)x;
+    }
+    const double coef = 2.0 * scale / ((double)nshot_norm * (double)NT * (double)NR);
+    for (int k = 0; k < sp.nsos; ++k) st[k][0] = st[k][1] = st[k][2] = st[k][3] = 0.0;
+    for (int n = g.nt - 1; n >= 0; --n) {
+        double x = coef * (double)cot[n * NR];
+        for (int k = sp.nsos - 1; k >= 0; --k) {
+            const double y = sp.c[k][0] * x + sp.c[k][1] * st[k][0] + sp.c[k][2] * st[k][1]
+                           - sp.c[k][3] * st[k][2] - sp.c[k][4] * st[k][3];
+            st[k][1] = st[k][0]; st[k][0] = x; st[k][3] = st[k][2]; st[k][2] = y;
+            x = y;
+        }
+        cot[n * NR] = (float)(taper(n) * x);
+    }
+    mis_trace[t] = scale / nshot_norm * sum / ((double)NT * (double)NR);
+}
+
+__global__ void k_misfit_reduce(int nshot, int nrec, const double *mis_trace, double *mis_shot)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshot) return;
+    double a = 0.0;
+    for (int r = 0; r < nrec; ++r) a += mis_trace[(long long)s * nrec + r];
+    mis_shot[s] = a;
+}
+
+// (M, L, L2M) or (lambda, mu) partial sums -> (Vs, Vp, rho) gradients on the
+// physical grid.  EXACT: M = rho Vs^2, L2M = rho Vp^2, L = L2M - 2M; the
+// free-surface ratio Lr = -L/L2M contributes on row 0.  IMAGING:
+// fwi/imaging.py:165-167.
+__global__ void k_finalize(Geo g, int groups, const double *acc, const double *accLr,
+                           const float *L2M, const float *L, const float *vs, const float *vp,
+                           const float *rho, int want_exact, int want_img, double *out_exact,
+                           double *out_img)
+{
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= g.nd) return;
+    const int pi = (int)(q / g.nx_dom), pj = (int)(q % g.nx_dom);
+    double gM = 0, gL = 0, gL2M = 0, gla = 0, gmu = 0;
+    for (int k = 0; k < groups; ++k) {
+        const double *a = acc + (long long)k * 5 * g.nd + q;
+        gM += a[0]; gL += a[g.nd]; gL2M += a[2 * g.nd]; gla += a[3 * g.nd]; gmu += a[4 * g.nd];
+    }
+    const double r = rho[q], a = vs[q], b = vp[q];
+    if (want_exact) {
+        if (g.fs && pi == 0) {
+            double glr = 0;
+            for (int k = 0; k < groups; ++k) glr += accLr[(long long)k * g.nx_dom + pj];
+            const long long o = (long long)(pi + g.z0) * g.P + pj + g.pad;
+            const double l2m = L2M[o], l = L[o];
+            gL += -glr / l2m;
+            gL2M += glr * l / (l2m * l2m);
+        }
+        out_exact[q] = 2.0 * r * a * (gM - 2.0 * gL);
+        out_exact[g.nd + q] = 2.0 * r * b * (gL2M + gL);
+        out_exact[2 * g.nd + q] = 0.0;
+    }
+    if (want_img) {
+        out_img[q] = 2.0 * r * a * (gmu - 2.0 * gla);
+        out_img[g.nd + q] = 2.0 * r * b * gla;
+        out_img[2 * g.nd + q] = (b * b - 2.0 * a * a) * gla + a * a * gmu;
+    }
+}
+
+// ---------------------------------------------------------------- launch helpers
+
+Mat mat_of(stfwi_handle *h)
+{
+    return Mat{h->B, h->L2M, h->L, h->M, h->Lr, h->bx, h->ax, h->ikx, h->bz, h->az, h->ikz};
+}
+Shots shots_of(stfwi_handle *h)
+{
+    return Shots{h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef, h->lm};
+}
+Recv recv_of(stfwi_handle *h) { return Recv{h->tile_start, h->tile_rec, h->rx, h->rz}; }
+
+// event pair of sampled step n around kernel k (0 fwd_vel, 1 fwd_str, 2 adj_a, 3 adj_b)
+inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
+{
+    if (h->prof_every <= 0 || n % h->prof_every) return;
+    const size_t idx = 2 * (size_t)(n / h->prof_every) + which;
+    if (idx < h->pev[k].size()) cudaEventRecord(h->pev[k][idx], st);
+}
+
+template <int FD>
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+{
+    // one shot per block: the forward carries no cross-shot state (the
+    // illumination sum uses FP64 atomics per cell and shot)
+    dim3 grid(h->g.tiles_x * h->g.tiles_z, h->nshot), block(TX, NWARP);
+    prof_mark(h, 0, n, 0, st);
+    k_fwd_vel<FD><<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, 1);
+    prof_mark(h, 0, n, 1, st);
+    prof_mark(h, 1, n, 0, st);
+    k_fwd_str<FD><<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->F, h->PX, h->PZ,
+                                          n, 1, o);
+    prof_mark(h, 1, n, 1, st);
+}
+
+template <int FD>
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+{
+    // U_a/V_a phase: one shot per block (no cross-shot state); strain phase:
+    // shot groups, so the FP64 gradient sum over shots stays in registers
+    dim3 grid_a(h->g.tiles_x * h->g.tiles_z, h->nshot), grid(h->g.tiles_x * h->g.tiles_z, h->groups);
+    dim3 block(TX, NWARP);
+    prof_mark(h, 2, n, 0, st);
+    k_adj_a<FD><<<grid_a, block, 0, st>>>(h->g, mat_of(h), recv_of(h), h->A, h->PX, h->PZ, n, 1, ai);
+    prof_mark(h, 2, n, 1, st);
+    prof_mark(h, 3, n, 0, st);
+    auto args = [&](auto kern) {
+        kern<<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spg, ao);
+    };
+    if (ao.want_exact && ao.want_img) args(k_adj_b<FD, true, true>);
+    else if (ao.want_exact) args(k_adj_b<FD, true, false>);
+    else if (ao.want_img) args(k_adj_b<FD, false, true>);
+    else {
+        dim3 grid1(h->g.tiles_x * h->g.tiles_z, h->nshot);
+        k_adj_b<FD, false, false><<<grid1, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX,
+                                                          h->PZ, n, 1, ao);
+    }
+    prof_mark(h, 3, n, 1, st);
+}
+
+
+
+stfwi_status zero_forward_state(stfwi_handle *h, cudaStream_t st)
+{
+    const Geo &g = h->g;
+    CK(h, cudaMemsetAsync(h->F, 0, (size_t)h->nshot * F_N * g.fstride * sizeof(float), st));
+    for (int s = 0; s < h->nshot; ++s) {
+        CK(h, cudaMemsetAsync(h->PX + (long long)s * NPX * g.xstride, 0,
+                              (size_t)PX_NFWD * g.xstride * sizeof(float), st));
+        CK(h, cudaMemsetAsync(h->PZ + (long long)s * NPZ * g.zstride, 0,
+                              (size_t)PZ_NFWD * g.zstride * sizeof(float), st));
+    }
+    CK(h, cudaMemsetAsync(h->status, 0, sizeof(int), st));
+    return STFWI_OK;
+}
+
+stfwi_status zero_adjoint_state(stfwi_handle *h, cudaStream_t st)
+{
+    const Geo &g = h->g;
+    CK(h, cudaMemsetAsync(h->A, 0, (size_t)h->nshot * F_N * g.fstride * sizeof(float), st));
+    for (int s = 0; s < h->nshot; ++s) {
+        CK(h, cudaMemsetAsync(h->PX + ((long long)s * NPX + PX_NFWD) * g.xstride, 0,
+                              (size_t)2 * PXA_N * g.xstride * sizeof(float), st));
+        CK(h, cudaMemsetAsync(h->PZ + ((long long)s * NPZ + PZ_NFWD) * g.zstride, 0,
+                              (size_t)2 * PZA_N * g.zstride * sizeof(float), st));
+    }
+    CK(h, cudaMemsetAsync(h->acc, 0, (size_t)h->groups * 5 * g.nd * sizeof(double), st));
+    CK(h, cudaMemsetAsync(h->accLr, 0, (size_t)h->groups * g.nx_dom * sizeof(double), st));
+    return STFWI_OK;
+}
+
+// record the whole forward pass (kind 0) or illumination pass (kind 2)
+stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStream_t st)
+{
+    stfwi_status rc = zero_forward_state(h, st);
+    if (rc) return rc;
+    FwdOut o{};
+    o.rec = h->rec;
+    o.status = h->status;
+    o.slots = h->slots;
+    const bool store = (flags & STFWI_FWD_STORE) != 0;
+    if (comp >= 0) {
+        CK(h, cudaMemsetAsync(h->energy, 0, (size_t)h->g.nz * h->g.nx * sizeof(double), st));
+        o.energy = h->energy;
+        o.energy_comp = comp;
+    }
+    for (int n = 0; n < h->g.nt; ++n) {
+        o.snap = store ? h->snap : nullptr;
+        o.row0 = (store && h->g.fs) ? h->row0 : nullptr;
+        o.slot = n;
+        switch (h->d.fd_order) {
+        case 2: launch_fwd_step<2>(h, n, o, st); break;
+        case 4: launch_fwd_step<4>(h, n, o, st); break;
+        default: launch_fwd_step<8>(h, n, o, st); break;
+        }
+    }
+    CK(h, cudaGetLastError());
+    return STFWI_OK;
+}
+
+// run `fn` on the handle's stream, ordered after `user` work, replaying a
+// captured graph when one exists for `key`
+template <class Fn>
+stfwi_status run_graph(stfwi_handle *h, GraphKey key, cudaStream_t user, Fn fn)
+{
+    CK(h, cudaEventRecord(h->ev_in, user));
+    CK(h, cudaStreamWaitEvent(h->hs, h->ev_in, 0));
+    auto it = h->graphs.find(key);
+    if (it == h->graphs.end()) {
+        cudaGraph_t graph = nullptr;
+        CK(h, cudaStreamBeginCapture(h->hs, cudaStreamCaptureModeThreadLocal));
+        stfwi_status rc = fn(h->hs);
+        cudaError_t e = cudaStreamEndCapture(h->hs, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return fail(h, STFWI_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        cudaGraphExec_t exec = nullptr;
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(h, STFWI_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        it = h->graphs.emplace(key, exec).first;
+    }
+    CK(h, cudaGraphLaunch(it->second, h->hs));
+    CK(h, cudaEventRecord(h->ev_out, h->hs));
+    CK(h, cudaStreamWaitEvent(user, h->ev_out, 0));
+    return STFWI_OK;
+}
+
+void drop_graphs(stfwi_handle *h)
+{
+    for (auto &kv : h->graphs) cudaGraphExecDestroy(kv.second);
+    h->graphs.clear();
+}
+
+// add the elapsed times of kernel kind k's sampled pairs (after its pass completed)
+void prof_accumulate(stfwi_handle *h, int k)
+{
+    for (size_t i = 0; i + 1 < h->pev[k].size(); i += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, h->pev[k][i], h->pev[k][i + 1]) == cudaSuccess) {
+            h->prof_ms[k] += ms;
+            h->prof_cnt[k] += 1;
+        }
+    }
+    cudaGetLastError();
+}
+
+}  // namespace
+
+// ================================================================ C ABI
+
+extern "C" {
+
+void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t)
+{
+    *nx_t = d->nx_dom + 2 * d->pad;
+    *nz_t = d->free_surface ? d->nz_dom + d->pad : d->nz_dom + 2 * d->pad;
+}
+
+size_t stfwi_workspace_bytes(const stfwi_desc *d)
+{
+    if (!d) return 0;
+    return make_plan(d).total();
+}
+
+const char *stfwi_last_error(const stfwi_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
+{
+    if (!d || !out) return STFWI_ERR_INVALID;
+    *out = nullptr;
+    if (d->fd_order != 2 && d->fd_order != 4 && d->fd_order != 8) return STFWI_ERR_UNSUPPORTED;
+    const int H = d->fd_order / 2;
+    if (d->nz_dom < 1 || d->nx_dom < 1 || d->pad < H || d->nt < 1 || d->nrec < 0 || d->max_shots < 1 ||
+        !(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0))
+        return STFWI_ERR_INVALID;
+    stfwi_handle *h = new stfwi_handle();
+    h->d = *d;
+    Plan p = make_plan(d);
+    cudaGetDevice(&h->device);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        delete h;
+        return STFWI_ERR_CUDA;
+    }
+    const double budget = d->mem_budget_gb > 0 ? d->mem_budget_gb * 1e9 : 0.85 * (double)fr;
+    if ((double)p.total() > budget) {
+        h->err = "workspace of " + std::to_string(p.total() / 1e9) + " GB exceeds the budget of " +
+                 std::to_string(budget / 1e9) + " GB";
+        fprintf(stderr, "stfwi_create: %s\n", h->err.c_str());
+        delete h;
+        return STFWI_ERR_OOM;
+    }
+    Geo &g = h->g;
+    g.nz = (int)p.nz; g.nx = (int)p.nx; g.P = (int)p.P;
+    g.nz_dom = d->nz_dom; g.nx_dom = d->nx_dom; g.z0 = d->free_surface ? 0 : d->pad; g.pad = d->pad;
+    g.fs = d->free_surface ? 1 : 0;
+    g.xs_n = (int)p.xs_n; g.zs_n = (int)p.zs_n;
+    g.nt = d->nt; g.nrec = d->nrec; g.nshot = 0;
+    g.tiles_x = p.tiles_x; g.tiles_z = p.tiles_z;
+    g.dtdx = (float)(d->dt / d->dx); g.dtdz = (float)(d->dt / d->dz); g.dzdx = (float)(d->dz / d->dx);
+    g.dt = (float)d->dt;
+    g.inv2dx = (float)(1.0 / (2.0 * d->dx)); g.inv2dz = (float)(1.0 / (2.0 * d->dz));
+    g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
+    h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
+    h->spg = (d->max_shots + h->groups - 1) / h->groups;
+    h->slots = d->nt;
+
+    auto alloc = [&](void **ptr, size_t bytes) -> bool {
+        if (bytes == 0) { *ptr = nullptr; return true; }
+        if (cudaMalloc(ptr, bytes) != cudaSuccess) return false;
+        h->bytes += bytes;
+        return true;
+    };
+    const long long S = d->max_shots, NP = p.nz * p.P, nd = p.nd;
+    const long long nrec = std::max(d->nrec, 1);
+    bool ok = true;
+    ok &= alloc((void **)&h->vs, nd * 4) && alloc((void **)&h->vp, nd * 4) && alloc((void **)&h->rho, nd * 4);
+    ok &= alloc((void **)&h->B, NP * 4) && alloc((void **)&h->L2M, NP * 4) && alloc((void **)&h->L, NP * 4) &&
+          alloc((void **)&h->M, NP * 4) && alloc((void **)&h->Lr, p.P * 4);
+    ok &= alloc((void **)&h->bx, p.P * 4) && alloc((void **)&h->ax, p.P * 4) && alloc((void **)&h->ikx, p.P * 4);
+    ok &= alloc((void **)&h->bz, p.nz * 4) && alloc((void **)&h->az, p.nz * 4) && alloc((void **)&h->ikz, p.nz * 4);
+    ok &= alloc((void **)&h->vpmax, 16) && alloc((void **)&h->status, 16);
+    ok &= alloc((void **)&h->sx, S * 4) && alloc((void **)&h->sz, S * 4) && alloc((void **)&h->stype, S * 4);
+    ok &= alloc((void **)&h->wav, S * d->nt * 4) && alloc((void **)&h->fcoef, S * 4) &&
+          alloc((void **)&h->mcoef, S * 4) && alloc((void **)&h->lm, S * 4);
+    ok &= alloc((void **)&h->tile_start, ((size_t)p.tiles_x * p.tiles_z + 1) * 4) &&
+          alloc((void **)&h->tile_rec, nrec * 4) && alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
+    ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
+    ok &= alloc((void **)&h->PX, (size_t)S * NPX * p.nz * p.xs_n * 4) &&
+          alloc((void **)&h->PZ, (size_t)S * NPZ * p.zs_n * p.P * 4);
+    ok &= alloc((void **)&h->rec, (size_t)S * 4 * d->nt * nrec * 4) &&
+          alloc((void **)&h->rec_adj, (size_t)S * 4 * d->nt * nrec * 4) &&
+          alloc((void **)&h->obs, (size_t)S * d->nt * nrec * 4);
+    ok &= alloc((void **)&h->snap, p.snap) && alloc((void **)&h->row0, p.row0);
+    ok &= alloc((void **)&h->acc, (size_t)h->groups * 5 * nd * 8) &&
+          alloc((void **)&h->accLr, (size_t)h->groups * std::max(d->nx_dom, 1) * 8) &&
+          alloc((void **)&h->gtmp, (size_t)6 * nd * 8);
+    ok &= alloc((void **)&h->energy, (size_t)p.nz * p.nx * 8);
+    ok &= alloc((void **)&h->mis_trace, (size_t)S * nrec * 8) && alloc((void **)&h->mis_shot, (size_t)S * 8);
+    ok &= alloc((void **)&h->src_a, (size_t)S * d->nt * 4);
+    if (!ok) {
+        cudaGetLastError();
+        stfwi_destroy(h);
+        return STFWI_ERR_OOM;
+    }
+    if (cudaStreamCreateWithFlags(&h->hs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+        stfwi_destroy(h);
+        return STFWI_ERR_CUDA;
+    }
+    cudaMemset(h->status, 0, 16);
+    *out = h;
+    return STFWI_OK;
+}
+
+void stfwi_destroy(stfwi_handle *h)
+{
+    if (!h) return;
+    if (h->hs) cudaStreamSynchronize(h->hs);
+    drop_graphs(h);
+    void *bufs[] = {h->vs, h->vp, h->rho, h->B, h->L2M, h->L, h->M, h->Lr, h->bx, h->ax, h->ikx, h->bz,
+                    h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
+                    h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
+                    h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
+                    h->mis_trace, h->mis_shot, h->src_a};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (int k = 0; k < 4; ++k)
+        for (cudaEvent_t e : h->pev[k]) cudaEventDestroy(e);
+    if (h->ev_in) cudaEventDestroy(h->ev_in);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->hs) cudaStreamDestroy(h->hs);
+    delete h;
+}
+
+stfwi_status stfwi_set_model(stfwi_handle *h, const float *vs, const float *vp, const float *rho,
+                             void *stream)
+{
+    if (!h || !vs || !vp || !rho) return fail(h, STFWI_ERR_INVALID, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    const size_t nb = (size_t)g.nd * sizeof(float);
+    CK(h, cudaMemcpyAsync(h->vs, vs, nb, cudaMemcpyDefault, st));
+    CK(h, cudaMemcpyAsync(h->vp, vp, nb, cudaMemcpyDefault, st));
+    CK(h, cudaMemcpyAsync(h->rho, rho, nb, cudaMemcpyDefault, st));
+    dim3 blk(128), grd((g.nx + 127) / 128, g.nz);
+    k_materials<<<grd, blk, 0, st>>>(g.nz, g.nx, g.P, g.nz_dom, g.nx_dom, g.z0, g.pad, h->vs, h->vp, h->rho,
+                                     h->B, h->L2M, h->L, h->M, h->Lr);
+    k_vpmax<<<1, 1024, 0, st>>>(h->vp, g.nd, h->vpmax);
+    const int nmax = std::max(g.nx, g.nz);
+    k_pml<<<(nmax + 127) / 128, 128, 0, st>>>(g.nz, g.nx, g.nz_dom, g.pad, g.fs, h->d.dx, h->d.dt, h->d.fc,
+                                              h->vpmax, h->bx, h->ax, h->ikx, h->bz, h->az, h->ikz);
+    CK(h, cudaGetLastError());
+    h->model_set = true;
+    if (h->shots_set) {
+        k_src_coefs<<<(h->nshot + 127) / 128, 128, 0, st>>>(h->nshot, h->sx, h->sz, g.P, h->B, h->L, h->M,
+                                                           (float)(h->d.dt / (h->d.dx * h->d.dz)),
+                                                           (float)h->d.dx, (float)h->d.dz, h->fcoef,
+                                                           h->mcoef, h->lm);
+        CK(h, cudaGetLastError());
+    }
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *rec_x, const int32_t *rec_z)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    const Geo &g = h->g;
+    if (nrec != g.nrec) return fail(h, STFWI_ERR_INVALID, "nrec %d != descriptor nrec %d", nrec, g.nrec);
+    if (nrec > 0 && (!rec_x || !rec_z)) return fail(h, STFWI_ERR_INVALID, "null receiver array");
+    const int ntile = g.tiles_x * g.tiles_z;
+    std::vector<int> rx(std::max(nrec, 1)), rz(std::max(nrec, 1)), cnt(ntile + 1, 0), start(ntile + 1, 0),
+        list(std::max(nrec, 1));
+    for (int r = 0; r < nrec; ++r) {
+        rx[r] = rec_x[r] + g.pad;
+        rz[r] = rec_z[r] + g.z0;
+        if (rx[r] < 0 || rx[r] >= g.nx || rz[r] < 0 || rz[r] >= g.nz)
+            return fail(h, STFWI_ERR_INVALID, "receiver %d at (%d,%d) is outside the grid", r, rec_z[r], rec_x[r]);
+        cnt[(rz[r] / TZ) * g.tiles_x + rx[r] / TX]++;
+    }
+    for (int t = 0; t < ntile; ++t) start[t + 1] = start[t] + cnt[t];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    for (int r = 0; r < nrec; ++r) list[fill[(rz[r] / TZ) * g.tiles_x + rx[r] / TX]++] = r;
+    CK(h, cudaMemcpy(h->rx, rx.data(), rx.size() * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->rz, rz.data(), rz.size() * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->tile_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->tile_rec, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
+    h->recv_set = true;
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src, const float *wavelets,
+                             void *stream)
+{
+    if (!h || !src || !wavelets) return fail(h, STFWI_ERR_INVALID, "null argument");
+    if (nshot < 1 || nshot > h->d.max_shots)
+        return fail(h, STFWI_ERR_INVALID, "nshot %d outside [1, %d]", nshot, h->d.max_shots);
+    cudaStream_t st = (cudaStream_t)stream;
+    Geo &g = h->g;
+    std::vector<int> sx(nshot), sz(nshot), ty(nshot);
+    for (int s = 0; s < nshot; ++s) {
+        sx[s] = src[3 * s] + g.pad;
+        sz[s] = src[3 * s + 1] + g.z0;
+        ty[s] = src[3 * s + 2];
+        if (ty[s] != STFWI_SRC_FORCE && ty[s] != STFWI_SRC_MOMENT)
+            return fail(h, STFWI_ERR_UNSUPPORTED, "src_type %d not supported (use force=0 or moment=1)", ty[s]);
+        if (sx[s] < 0 || sx[s] >= g.nx || sz[s] < 0 || sz[s] >= g.nz)
+            return fail(h, STFWI_ERR_INVALID, "source %d at (%d,%d) is outside the grid", s, src[3 * s + 1], src[3 * s]);
+    }
+    CK(h, cudaStreamSynchronize(st));
+    CK(h, cudaMemcpy(h->sx, sx.data(), nshot * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->sz, sz.data(), nshot * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->stype, ty.data(), nshot * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpyAsync(h->wav, wavelets, (size_t)nshot * g.nt * 4, cudaMemcpyDefault, st));
+    if (nshot != h->nshot) drop_graphs(h);
+    h->nshot = nshot;
+    g.nshot = nshot;
+    h->spg = std::max(1, (nshot + h->groups - 1) / h->groups);
+    h->shots_set = true;
+    h->stored = false;
+    if (h->model_set) {
+        k_src_coefs<<<(nshot + 127) / 128, 128, 0, st>>>(nshot, h->sx, h->sz, g.P, h->B, h->L, h->M,
+                                                        (float)(h->d.dt / (h->d.dx * h->d.dz)),
+                                                        (float)h->d.dx, (float)h->d.dz, h->fcoef, h->mcoef,
+                                                        h->lm);
+        CK(h, cudaGetLastError());
+    }
+    return STFWI_OK;
+}
+
+static stfwi_status ready(stfwi_handle *h)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    if (!h->model_set || !h->shots_set || !h->recv_set)
+        return fail(h, STFWI_ERR_STATE, "set the model, receivers and shots first");
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_forward(stfwi_handle *h, uint32_t flags, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if ((flags & STFWI_FWD_STORE) && !h->snap)
+        return fail(h, STFWI_ERR_STATE, "handle was created without want_gradient");
+    GraphKey key{0, flags & STFWI_FWD_STORE, h->nshot};
+    rc = run_graph(h, key, (cudaStream_t)stream,
+                   [&](cudaStream_t st) { return enqueue_forward(h, flags, -1, st); });
+    if (rc) return rc;
+    h->stored = (flags & STFWI_FWD_STORE) != 0;
+    if (h->prof_every > 0) {
+        CK(h, cudaStreamSynchronize(h->hs));
+        prof_accumulate(h, 0);
+        prof_accumulate(h, 1);
+    }
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_get_records(stfwi_handle *h, float *out, void *stream)
+{
+    if (!h || !out) return fail(h, STFWI_ERR_INVALID, "null argument");
+    CK(h, cudaMemcpyAsync(out, h->rec, (size_t)h->nshot * 4 * h->g.nt * h->g.nrec * 4, cudaMemcpyDefault,
+                          (cudaStream_t)stream));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_misfit(stfwi_handle *h, const float *obs, const stfwi_misfit_desc *m,
+                          double *misfit_out, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if (!obs || !m) return fail(h, STFWI_ERR_INVALID, "null argument");
+    if (m->component < 0 || m->component > 3) return fail(h, STFWI_ERR_INVALID, "component %d", m->component);
+    if (m->nsos < 0 || m->nsos > MAX_SOS || (m->nsos > 0 && !m->sos))
+        return fail(h, STFWI_ERR_INVALID, "nsos %d outside [0, %d]", m->nsos, MAX_SOS);
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    SosParams sp{};
+    sp.nsos = m->nsos;
+    for (int k = 0; k < m->nsos; ++k) {
+        const double *s = m->sos + 6 * k;
+        if (s[3] == 0.0) return fail(h, STFWI_ERR_INVALID, "sos section %d has a0 = 0", k);
+        sp.c[k][0] = s[0] / s[3]; sp.c[k][1] = s[1] / s[3]; sp.c[k][2] = s[2] / s[3];
+        sp.c[k][3] = s[4] / s[3]; sp.c[k][4] = s[5] / s[3];
+    }
+    const int nnorm = m->reserved > 0 ? m->reserved : h->nshot;
+    CK(h, cudaMemcpyAsync(h->obs, obs, (size_t)h->nshot * g.nt * g.nrec * 4, cudaMemcpyDefault, st));
+    const int n = h->nshot * g.nrec, thr = 128;
+    if (n > 0) {
+        const int ntap = std::min(std::max(m->n_taper, 0), g.nt);  // fwi/filters.py:28
+        k_misfit<<<(n + thr - 1) / thr, thr, 0, st>>>(g, m->component, ntap, sp, m->scale, nnorm, h->rec,
+                                                     h->obs, h->rec_adj, h->mis_trace);
+        k_misfit_reduce<<<(h->nshot + 127) / 128, 128, 0, st>>>(h->nshot, g.nrec, h->mis_trace, h->mis_shot);
+    } else {
+        CK(h, cudaMemsetAsync(h->mis_shot, 0, h->nshot * 8, st));
+    }
+    CK(h, cudaGetLastError());
+    if (misfit_out) CK(h, cudaMemcpyAsync(misfit_out, h->mis_shot, h->nshot * 8, cudaMemcpyDefault, st));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_adjoint_sources(stfwi_handle *h, const float *rec_adj, void *stream)
+{
+    if (!h || !rec_adj) return fail(h, STFWI_ERR_INVALID, "null argument");
+    CK(h, cudaMemcpyAsync(h->rec_adj, rec_adj, (size_t)h->nshot * 4 * h->g.nt * h->g.nrec * 4,
+                          cudaMemcpyDefault, (cudaStream_t)stream));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float *src_wav_a, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    const bool ex = mode & STFWI_GRAD_EXACT, im = mode & STFWI_GRAD_IMAGING, sr = mode & STFWI_GRAD_SRC;
+    if (!ex && !im && !sr) return fail(h, STFWI_ERR_INVALID, "empty gradient mode");
+    if ((ex || im) && !g_out) return fail(h, STFWI_ERR_INVALID, "g_out is null");
+    if (sr && !src_wav_a) return fail(h, STFWI_ERR_INVALID, "src_wav_a is null");
+    if ((ex || im) && !h->stored)
+        return fail(h, STFWI_ERR_STATE, "model gradients need a preceding stfwi_forward(STFWI_FWD_STORE)");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    float *src_dev = sr ? h->src_a : nullptr;
+    GraphKey key{1, mode, h->nshot};
+    rc = run_graph(h, key, st, [&](cudaStream_t s) {
+        stfwi_status r = zero_adjoint_state(h, s);
+        if (r) return r;
+        const int thr = 256;
+        if (g.nrec > 0)
+            k_inject_last<<<(g.nshot * g.nrec + thr - 1) / thr, thr, 0, s>>>(g, h->rx, h->rz, h->rec_adj, h->A);
+        for (int n = g.nt - 1; n >= 0; --n) {
+            const int ping = (g.nt - 1 - n) & 1;
+            AdjIn ai{};
+            ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = n;
+            ai.accLr = h->accLr; ai.want_exact = ex; ai.ping = ping;
+            AdjOut ao{};
+            ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = n - 1; ao.slot_img = n;
+            ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im;
+            ao.src_a = sr ? src_dev : nullptr; ao.rec_adj = h->rec_adj; ao.ping = ping;
+            switch (h->d.fd_order) {
+            case 2: launch_adj_step<2>(h, n, ai, ao, s); break;
+            case 4: launch_adj_step<4>(h, n, ai, ao, s); break;
+            default: launch_adj_step<8>(h, n, ai, ao, s); break;
+            }
+        }
+        if (ex || im)
+            k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->groups, h->acc, h->accLr, h->L2M,
+                                                                      h->L, h->vs, h->vp, h->rho, ex, im,
+                                                                      h->gtmp, h->gtmp + 3 * g.nd);
+        CK(h, cudaGetLastError());
+        return STFWI_OK;
+    });
+    if (rc) return rc;
+    if (h->prof_every > 0) {
+        CK(h, cudaStreamSynchronize(h->hs));
+        prof_accumulate(h, 2);
+        prof_accumulate(h, 3);
+    }
+    if (sr) CK(h, cudaMemcpyAsync(src_wav_a, src_dev, (size_t)h->nshot * g.nt * 4, cudaMemcpyDefault, st));
+    size_t off = 0;
+    if (ex) {
+        CK(h, cudaMemcpyAsync(g_out, h->gtmp, (size_t)3 * g.nd * 8, cudaMemcpyDefault, st));
+        off += 3 * g.nd;
+    }
+    if (im) CK(h, cudaMemcpyAsync(g_out + off, h->gtmp + 3 * g.nd, (size_t)3 * g.nd * 8, cudaMemcpyDefault, st));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_illumination(stfwi_handle *h, int32_t component, double *ws_out, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if (component < 0 || component > 3 || !ws_out) return fail(h, STFWI_ERR_INVALID, "bad illumination request");
+    GraphKey key{2, (uint32_t)component, h->nshot};
+    rc = run_graph(h, key, (cudaStream_t)stream,
+                   [&](cudaStream_t st) { return enqueue_forward(h, 0, component, st); });
+    if (rc) return rc;
+    h->stored = false;
+    CK(h, cudaMemcpyAsync(ws_out, h->energy, (size_t)h->g.nz * h->g.nx * 8, cudaMemcpyDefault,
+                          (cudaStream_t)stream));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_profile(stfwi_handle *h, int32_t every)
+{
+    if (!h || every < 0) return STFWI_ERR_INVALID;
+    CK(h, cudaStreamSynchronize(h->hs));
+    drop_graphs(h);
+    for (int k = 0; k < 4; ++k) {
+        for (cudaEvent_t e : h->pev[k]) cudaEventDestroy(e);
+        h->pev[k].clear();
+        h->prof_ms[k] = 0;
+        h->prof_cnt[k] = 0;
+    }
+    h->prof_every = every;
+    if (every > 0) {
+        const int ns = (h->g.nt + every - 1) / every;
+        for (int k = 0; k < 4; ++k) {
+            h->pev[k].resize(2 * (size_t)ns);
+            for (auto &e : h->pev[k]) CK(h, cudaEventCreate(&e));
+        }
+    }
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out)
+{
+    if (!h || !out) return STFWI_ERR_INVALID;
+    CK(h, cudaStreamSynchronize(h->hs));
+    for (int k = 0; k < 4; ++k) {
+        out[2 * k] = h->prof_ms[k];
+        out[2 * k + 1] = (double)h->prof_cnt[k];
+        h->prof_ms[k] = 0;
+        h->prof_cnt[k] = 0;
+    }
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_check(stfwi_handle *h, void *stream)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    int v = 0;
+    CK(h, cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(h, cudaStreamSynchronize((cudaStream_t)stream));
+    if (v & 1) return fail(h, STFWI_ERR_NONFINITE, "a receiver sample became non-finite (unstable dt or model?)");
+    return STFWI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,223 @@
+"""Host-side handle over the C ABI: one padded grid, one shot batch, one GPU.
+
+Arrays may be NumPy (host) or torch tensors (host or CUDA); the C ABI copies
+with cudaMemcpyDefault, so device tensors never leave the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _native as N
+
+SRC_TYPES = {"force": N.SRC_FORCE, "moment": N.SRC_MOMENT}
+
+
+def _torch():
+    try:
+        import torch
+        return torch
+    except ImportError:  # pragma: no cover
+        return None
+
+
+def _as_buffer(x, dtype):
+    """(pointer, keep-alive) for a host or device array of the given dtype."""
+    t = _torch()
+    if t is not None and isinstance(x, t.Tensor):
+        tdt = {np.float32: t.float32, np.float64: t.float64, np.int32: t.int32}[dtype]
+        x = x.detach().to(tdt).contiguous()
+        return x.data_ptr(), x
+    a = np.ascontiguousarray(np.asarray(x, dtype=dtype))
+    return a.ctypes.data, a
+
+
+def _stream():
+    t = _torch()
+    if t is not None and t.cuda.is_available() and t.cuda.is_initialized():
+        return ct.c_void_p(t.cuda.current_stream().cuda_stream)
+    return None
+
+
+class Solver:
+    """Batch of shots on one model; mirrors the arguments of the reference's
+    forward_jax / build_forward_fn (fwi/forward.py:119-123, :508-509)."""
+
+    def __init__(self, nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, max_shots, fd_order=2,
+                 free_surface=True, want_gradient=True, shot_group=0, mem_budget_gb=0.0):
+        if fd_order not in (2, 4, 8):
+            raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
+        self.lib = N.load()
+        self.desc = N.StfwiDesc(int(nz_dom), int(nx_dom), int(pad), int(fd_order),
+                                int(bool(free_surface)), int(nt), int(nrec), int(max_shots),
+                                float(dx), float(dz), float(dt), float(fc), int(bool(want_gradient)),
+                                int(shot_group), float(mem_budget_gb))
+        h = ct.c_void_p()
+        st = self.lib.stfwi_create(ct.byref(self.desc), ct.byref(h))
+        if st != N.STFWI_OK:
+            raise N.StfwiError(st, f"stfwi_create failed for {self.shape_desc()}")
+        self.h = h
+        self.nz_dom, self.nx_dom, self.nt, self.nrec = int(nz_dom), int(nx_dom), int(nt), int(nrec)
+        self.pad, self.free_surface, self.fd_order = int(pad), bool(free_surface), int(fd_order)
+        nzt, nxt = ct.c_int32(), ct.c_int32()
+        self.lib.stfwi_grid_shape(ct.byref(self.desc), ct.byref(nzt), ct.byref(nxt))
+        self.nz, self.nx = nzt.value, nxt.value
+        self.nshot = 0
+
+    def shape_desc(self):
+        d = self.desc
+        return (f"grid {d.nz_dom}x{d.nx_dom} pad {d.pad} fd{d.fd_order} nt {d.nt} nrec {d.nrec} "
+                f"shots {d.max_shots}")
+
+    @staticmethod
+    def workspace_bytes(**kw):
+        lib = N.load()
+        d = N.StfwiDesc(kw["nz_dom"], kw["nx_dom"], kw["pad"], kw.get("fd_order", 2),
+                        int(kw.get("free_surface", True)), kw["nt"], kw["nrec"], kw["max_shots"],
+                        kw["dx"], kw["dz"], kw["dt"], kw["fc"], int(kw.get("want_gradient", True)),
+                        kw.get("shot_group", 0), kw.get("mem_budget_gb", 0.0))
+        return int(lib.stfwi_workspace_bytes(ct.byref(d)))
+
+    # ------------------------------------------------------------------ helpers
+    def _ok(self, st, what):
+        if st != N.STFWI_OK:
+            msg = self.lib.stfwi_last_error(self.h).decode()
+            if st == N.STFWI_ERR_UNSUPPORTED:
+                raise NotImplementedError(f"{what}: {msg}")
+            if st == N.STFWI_ERR_INVALID:
+                raise ValueError(f"{what}: {msg}")
+            raise N.StfwiError(st, f"{what}: {msg}")
+
+    def check(self):
+        self._ok(self.lib.stfwi_check(self.h, _stream()), "stfwi_check")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.stfwi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ set-up
+    def set_model(self, Vs, Vp, rho):
+        for name, a in (("Vs", Vs), ("Vp", Vp), ("rho", rho)):
+            if tuple(a.shape) != (self.nz_dom, self.nx_dom):
+                raise ValueError(f"{name} has shape {tuple(a.shape)}, expected {(self.nz_dom, self.nx_dom)}")
+        p1, k1 = _as_buffer(Vs, np.float32)
+        p2, k2 = _as_buffer(Vp, np.float32)
+        p3, k3 = _as_buffer(rho, np.float32)
+        self._ok(self.lib.stfwi_set_model(self.h, p1, p2, p3, _stream()), "set_model")
+        self._model_keep = (k1, k2, k3)
+
+    def set_receivers(self, rec_x, rec_z):
+        rx = np.ascontiguousarray(np.asarray(rec_x, dtype=np.int32).reshape(-1))
+        rz = np.ascontiguousarray(np.asarray(rec_z, dtype=np.int32).reshape(-1))
+        if rx.size != self.nrec or rz.size != self.nrec:
+            raise ValueError(f"expected {self.nrec} receivers, got {rx.size}/{rz.size}")
+        self._ok(self.lib.stfwi_set_receivers(self.h, self.nrec, rx.ctypes.data, rz.ctypes.data),
+                 "set_receivers")
+
+    def set_shots(self, src_x, src_z, src_types, wavelets):
+        sx = np.asarray(src_x, dtype=np.int64).reshape(-1)
+        sz = np.asarray(src_z, dtype=np.int64).reshape(-1)
+        if isinstance(src_types, str):
+            src_types = [src_types] * sx.size
+        try:
+            ty = [SRC_TYPES[t] if isinstance(t, str) else int(t) for t in src_types]
+        except KeyError as e:
+            raise NotImplementedError(f"src_type={e.args[0]!r} not supported (use 'force' or 'moment').")
+        src = np.ascontiguousarray(np.stack([sx, sz, np.asarray(ty)], axis=1).astype(np.int32))
+        w = wavelets
+        if getattr(w, "ndim", 1) == 1:
+            w = np.broadcast_to(np.asarray(w, dtype=np.float32), (sx.size, self.nt))
+        if tuple(w.shape) != (sx.size, self.nt):
+            raise ValueError(f"wavelets have shape {tuple(w.shape)}, expected {(sx.size, self.nt)}")
+        pw, kw = _as_buffer(w, np.float32)
+        self._ok(self.lib.stfwi_set_shots(self.h, int(sx.size), src.ctypes.data, pw, _stream()),
+                 "set_shots")
+        self._shots_keep = (src, kw)
+        self.nshot = int(sx.size)
+
+    # ------------------------------------------------------------------ passes
+    def forward(self, store=False):
+        self._ok(self.lib.stfwi_forward(self.h, N.FWD_STORE if store else 0, _stream()), "forward")
+
+    def records(self, out=None):
+        """[nshot, 4, nt, nrec] float32 receiver traces (vx, vz, exx, ezz)."""
+        if out is None:
+            out = np.empty((self.nshot, 4, self.nt, self.nrec), dtype=np.float32)
+        p, keep = _as_buffer(out, np.float32) if not isinstance(out, np.ndarray) else (out.ctypes.data, out)
+        self._ok(self.lib.stfwi_get_records(self.h, p, _stream()), "get_records")
+        self.check()
+        return keep if not isinstance(out, np.ndarray) else out
+
+    def misfit(self, obs, component, scale=1.0, sos=None, n_taper=0, nshot_norm=0, out=None, sync=True):
+        """Per-shot misfit terms (FP64) and, inside the handle, the adjoint
+        sources.  ``out`` may be a device tensor of nshot float64."""
+        po, ko = _as_buffer(obs, np.float32)
+        sos_a = None if sos is None else np.ascontiguousarray(np.asarray(sos, dtype=np.float64))
+        m = N.StfwiMisfitDesc(int(component), int(n_taper), 0 if sos_a is None else sos_a.shape[0],
+                              int(nshot_norm), float(scale),
+                              None if sos_a is None else sos_a.ctypes.data_as(ct.POINTER(ct.c_double)))
+        if out is None:
+            out = np.zeros(self.nshot, dtype=np.float64)
+        ptr = out.ctypes.data if isinstance(out, np.ndarray) else out.data_ptr()
+        self._ok(self.lib.stfwi_misfit(self.h, po, ct.byref(m), ptr, _stream()), "misfit")
+        if sync:
+            self.check()
+        self._obs_keep = ko
+        return out
+
+    def set_adjoint_sources(self, rec_adj):
+        p, keep = _as_buffer(rec_adj, np.float32)
+        self._ok(self.lib.stfwi_set_adjoint_sources(self.h, p, _stream()), "set_adjoint_sources")
+        self.check()
+        del keep
+
+    def gradient(self, exact=True, imaging=False, src=False, out=None, sync=True):
+        """Adjoint sweep.  Returns a dict with 'exact' / 'imaging' ->
+        (g_Vs, g_Vp, g_rho) FP64 arrays and 'src' -> [nshot, nt] float32.
+        ``out`` may be a device tensor [n_modes, 3, nz_dom, nx_dom] float64."""
+        mode = (N.GRAD_EXACT if exact else 0) | (N.GRAD_IMAGING if imaging else 0) | (N.GRAD_SRC if src else 0)
+        nmat = int(exact) + int(imaging)
+        g = out if out is not None else np.zeros((max(nmat, 1), 3, self.nz_dom, self.nx_dom), dtype=np.float64)
+        gptr = g.ctypes.data if isinstance(g, np.ndarray) else g.data_ptr()
+        sa = np.zeros((max(self.nshot, 1), self.nt), dtype=np.float32)
+        self._ok(self.lib.stfwi_gradient(self.h, mode, gptr if nmat else None,
+                                         sa.ctypes.data if src else None, _stream()), "gradient")
+        if sync or src:
+            self.check()
+        out = {}
+        k = 0
+        if exact:
+            out["exact"] = tuple(g[k]); k += 1
+        if imaging:
+            out["imaging"] = tuple(g[k]); k += 1
+        if src:
+            out["src"] = sa
+        return out
+
+    KERNELS = ("fwd_vel", "fwd_str", "adj_a", "adj_b")
+
+    def profile(self, every):
+        """Sample a CUDA-event pair around each kernel of every `every`-th step."""
+        self._ok(self.lib.stfwi_profile(self.h, int(every)), "profile")
+
+    def kernel_times(self):
+        """{kernel: (total ms, launches)} of the sampled launches since the last call."""
+        out = np.zeros(8, dtype=np.float64)
+        self._ok(self.lib.stfwi_kernel_times(self.h, out.ctypes.data), "kernel_times")
+        return {k: (float(out[2 * i]), int(out[2 * i + 1])) for i, k in enumerate(self.KERNELS)}
+
+    def illumination(self, component):
+        """Sum over shots and steps of field**2 on the padded grid (FP64)."""
+        ws = np.zeros((self.nz, self.nx), dtype=np.float64)
+        self._ok(self.lib.stfwi_illumination(self.h, int(component), ws.ctypes.data, _stream()),
+                 "illumination")
+        self.check()
+        return ws

@@ -1,0 +1,125 @@
+"""CUDA path vs the oracle and the reference's known answers (B200).
+
+Tolerances (FP32 stencils against FP64 references):
+* seismograms: rel-L2 <= 1e-5 on the 60-step dot-product cases
+  (observed ~1e-7; bound from FP32 rounding growth over the steps);
+* dot-product identity in FP32: |<Ls,y> - <s,L^T y>| / |<Ls,y>| <= 1e-5;
+* Marmousi 5 shots x 400 steps: misfit rel <= 1e-4, g_Vs rel-L2 <= 1e-3
+  against the reference's FP64 AD gradient and imaging gradient.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import dot_case as C
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx=C.NX, dx=C.DX,
+            dz=C.DZ, dt=C.DT, fc=C.FC, **kw):
+    from stfwi_b200 import Solver
+    return Solver(nz, nx, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order=fd, free_surface=fs,
+                  want_gradient=want_gradient, **kw)
+
+
+@pytest.mark.parametrize("fd,fs,st", C.CONFIGS)
+def test_forward_and_adjoint_vs_oracle(fd, fs, st):
+    """The reference's dot-product case (test_adjoint_kernel.py) on the GPU:
+    seismograms and the source adjoint against the FP64 oracle, and the
+    dot-product identity of the FP32 kernels."""
+    vs, vp, rho = C.model()
+    sx, sz, rx, rz = C.acquisition(fs, st)
+    s_in, ys = C.random_vectors()
+    S = _solver(C.NT, len(rx), 1, fd, fs)
+    S.set_model(vs, vp, rho)
+    S.set_receivers(rx, rz)
+    S.set_shots([sx], [sz], [st], s_in.astype(np.float32))
+    S.forward()
+    rec = S.records()[0]
+    ref, _, _ = O.forward(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, C.NT, C.FC,
+                          C.PAD, s_in, fd, fs, st, d0_f32=True)
+    for c in range(4):
+        assert _rel(rec[c], ref[c]) < 1e-5, (c, _rel(rec[c], ref[c]))
+    S.set_adjoint_sources(np.stack(ys)[None].astype(np.float32))
+    src_a = S.gradient(exact=False, src=True)["src"][0]
+    a = O.adjoint(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, C.NT, C.FC, C.PAD, *ys,
+                  fd_order=fd, free_surface=fs, src_type=st, d0_f32=True)
+    assert _rel(src_a, a["src"]) < 1e-5, _rel(src_a, a["src"])
+    lhs = sum(float(np.sum(rec[c].astype(np.float64) * ys[c])) for c in range(4))
+    rhs = float(np.sum(s_in * src_a.astype(np.float64)))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5, (lhs, rhs)
+    S.close()
+
+
+@pytest.mark.parametrize("fd,fs,st", [(8, True, "force"), (8, True, "moment"), (4, False, "force"),
+                                      (2, False, "moment")])
+def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st):
+    """Model gradients of the GPU (FP32 stencils, FP64 sums) against the
+    FP64 oracle on a small case: exact (AD) and imaging formula."""
+    vs, vp, rho = C.model()
+    nt = 120
+    sx, sz, rx, rz = C.acquisition(fs, st)
+    wav = O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9
+    geo = dict(rec_x=rx, rec_z=rz, nx_dom=C.NX, nz_dom=C.NZ, dx=C.DX, dz=C.DZ, dt=C.DT, nt=nt,
+               fc=C.FC, pad=C.PAD, fd_order=fd, free_surface=fs, d0_f32=True)
+    obs = O.forward_batch(vs * 1.03, vp, rho, [sx], [sz], [st], src_wavelet=wav, **geo)[:, 0]
+    kw = dict(src_x=[sx], src_z=[sz], src_wavelet=wav, observed=obs, src_types=[st], component=0,
+              scale=1.0, invert="vs_vp", **geo)
+    (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
+    (gi_vs, gi_vp, _), _ = O.compute_gradient("adjoint", Vs=vs, Vp=vp, rho=rho, **kw)
+    S = _solver(nt, len(rx), 1, fd, fs, want_gradient=True)
+    S.set_model(vs, vp, rho)
+    S.set_receivers(rx, rz)
+    S.set_shots([sx], [sz], [st], wav.astype(np.float32))
+    S.forward(store=True)
+    mis = S.misfit(obs.astype(np.float32), 0, 1.0)
+    # the misfit is a sum of squared differences of nearly equal traces; its
+    # FP32 error scales with |pred| / |pred - obs|
+    rec = S.records()[0, 0].astype(np.float64)
+    amp = float(np.linalg.norm(rec) / np.linalg.norm(rec - obs[0]))
+    g = S.gradient(exact=True, imaging=True)
+    errs = {"misfit": abs(mis.sum() / loss - 1),
+            "exact_vs": _rel(g["exact"][0], gx_vs), "exact_vp": _rel(g["exact"][1], gx_vp),
+            "img_vs": _rel(g["imaging"][0], gi_vs), "img_vp": _rel(g["imaging"][1], gi_vp)}
+    print(f"fd{fd} fs={fs} {st}: amplification {amp:.1f} errors {errs}")
+    tol = 2e-5 * max(amp, 1.0)
+    assert all(e < tol for e in errs.values()), (tol, errs)
+    S.close()
+
+
+def test_marmousi_known_answers(known_answers):
+    """Results_gradient/gradient_compare.npz: 5 shots, nt=400, fd8, free
+    surface, exx misfit.  FP32 GPU against the reference's FP64 numbers."""
+    K = known_answers
+    nt, pad, fd = int(K["gc_nt"]), int(K["gc_pad"]), int(K["gc_fd_order"])
+    dt, fc, comp = float(K["gc_dt"]), float(K["gc_f_c"]), int(K["gc_component"])
+    nz, nx = K["Vs_true"].shape
+    rx, rz = K["gc_rec_x"], K["gc_rec_z"]
+    ns = len(K["gc_src_x"])
+    wav = O.ricker(np.arange(nt) * dt, fc, 1.5 / fc).astype(np.float32)
+    S = _solver(nt, len(rx), ns, fd, True, want_gradient=True, pad=pad, nz=nz, nx=nx, dx=20.0,
+                dz=20.0, dt=dt, fc=fc)
+    S.set_receivers(rx, rz)
+    S.set_shots(K["gc_src_x"], K["gc_src_z"], "force", wav)
+    S.set_model(K["Vs_true"], K["Vp_true"], K["rho_true"])
+    S.forward()
+    obs = S.records()[:, comp].copy()
+    auto = 1.0 / (np.mean(obs.astype(np.float64) ** 2) + 1e-45)
+    assert abs(auto / K["gc_auto_scale"] - 1) < 1e-4, (auto, K["gc_auto_scale"])
+    S.set_model(K["Vs_init"], K["Vp_init"], K["rho_init"])
+    S.forward(store=True)
+    loss = S.misfit(obs, comp, float(K["gc_auto_scale"])).sum()
+    assert abs(loss / K["gc_loss_AD"] - 1) < 1e-4, (loss, K["gc_loss_AD"])
+    g = S.gradient(exact=True, imaging=True)
+    e_ad = _rel(g["exact"][0], K["gc_g_Vs_AD"])
+    e_hc = _rel(g["imaging"][0], K["gc_g_Vs_HC"])
+    print(f"marmousi: loss rel {abs(loss / K['gc_loss_AD'] - 1):.3e}  g_Vs_AD rel-L2 {e_ad:.3e}  "
+          f"g_Vs_HC rel-L2 {e_hc:.3e}")
+    assert e_ad < 1e-3 and e_hc < 1e-3, (e_ad, e_hc)
+    S.close()
