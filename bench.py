@@ -260,6 +260,11 @@ def main():
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tot_ms = 0.0
+    # STFWI_PROFILER_RANGE=1 marks the timed region for a profiler started
+    # with its collection off (ncu --profile-from-start off)
+    mark = os.environ.get("STFWI_PROFILER_RANGE") == "1"
+    if mark:
+        torch.cuda.cudart().cudaProfilerStart()
     with Clocks(local) as clk:
         for _ in range(args.steps):
             flush_l2()
@@ -268,6 +273,8 @@ def main():
             ev1.record(stream)
             ev1.synchronize()
             tot_ms += ev0.elapsed_time(ev1)
+    if mark:
+        torch.cuda.cudart().cudaProfilerStop()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -324,8 +331,8 @@ def main():
     kb = kernel_bytes(cfg, ns)
     dom = max(ktimes, key=lambda k: ktimes[k][0])
     tot, cnt = ktimes[dom]
-    avg_ms = tot / max(cnt, 1)
-    achieved = kb[dom] / (avg_ms * 1e-3) / 1e9
+    avg_ms = tot / cnt if cnt else float("nan")
+    achieved = kb[dom] / (avg_ms * 1e-3) / 1e9 if cnt and avg_ms > 0 else float("nan")
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": None,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",

@@ -368,7 +368,8 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
 {
     if (h->prof_every <= 0 || n % h->prof_every) return;
     const size_t idx = 2 * (size_t)(n / h->prof_every) + which;
-    if (idx < h->pev[k].size()) cudaEventRecord(h->pev[k][idx], st);
+    // inside stream capture only an external record becomes an event node of the graph
+    if (idx < h->pev[k].size()) cudaEventRecordWithFlags(h->pev[k][idx], st, cudaEventRecordExternal);
 }
 
 template <int FD>
