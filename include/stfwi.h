@@ -42,7 +42,8 @@ typedef enum {
     STFWI_ERR_CUDA = 3,        /* a CUDA runtime call failed */
     STFWI_ERR_OOM = 4,         /* workspace does not fit the memory budget */
     STFWI_ERR_NONFINITE = 5,   /* a receiver sample became NaN/Inf (unstable model or dt) */
-    STFWI_ERR_STATE = 6        /* call order: e.g. gradient before a storing forward */
+    STFWI_ERR_STATE = 6,       /* call order: e.g. gradient before a storing forward */
+    STFWI_ERR_TIMEOUT = 7      /* a kernel's bounded wait on a tile copy expired */
 } stfwi_status;
 
 typedef struct stfwi_handle stfwi_handle;
@@ -61,6 +62,8 @@ typedef struct {
     int32_t want_gradient;  /* 1: reserve strain history + accumulators */
     int32_t shot_group;     /* shots per block (0: automatic) */
     double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
+    int32_t kernel_variant; /* 0: TMA-pipelined tiles (default), 1: plain shared-memory tiles */
+    int32_t reserved0;
 } stfwi_desc;
 
 /* source types */

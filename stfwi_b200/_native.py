@@ -8,11 +8,13 @@ import ctypes as ct
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libstfwi.so")
+# STFWI_LIB selects another build of the same C ABI (e.g. a tuning variant)
+LIB_PATH = os.environ.get("STFWI_LIB") or os.path.join(HERE, "libstfwi.so")
 
 STFWI_OK, STFWI_ERR_INVALID, STFWI_ERR_UNSUPPORTED, STFWI_ERR_CUDA = 0, 1, 2, 3
-STFWI_ERR_OOM, STFWI_ERR_NONFINITE, STFWI_ERR_STATE = 4, 5, 6
-STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "OOM", 5: "NONFINITE", 6: "STATE"}
+STFWI_ERR_OOM, STFWI_ERR_NONFINITE, STFWI_ERR_STATE, STFWI_ERR_TIMEOUT = 4, 5, 6, 7
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CUDA", 4: "OOM", 5: "NONFINITE", 6: "STATE",
+                7: "TIMEOUT"}
 
 SRC_FORCE, SRC_MOMENT = 0, 1
 FWD_STORE = 1
@@ -34,6 +36,7 @@ class StfwiDesc(ct.Structure):
         ("nrec", ct.c_int32), ("max_shots", ct.c_int32),
         ("dx", ct.c_double), ("dz", ct.c_double), ("dt", ct.c_double), ("fc", ct.c_double),
         ("want_gradient", ct.c_int32), ("shot_group", ct.c_int32), ("mem_budget_gb", ct.c_double),
+        ("kernel_variant", ct.c_int32), ("reserved0", ct.c_int32),
     ]
 
 

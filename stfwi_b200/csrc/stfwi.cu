@@ -1,6 +1,8 @@
 // C ABI of the B200 elastic velocity-strain solver: handle, workspace plan,
 // model/geometry set-up kernels, launch sequences (captured into CUDA graphs)
 // and the residual/misfit kernel.  Declarations: include/stfwi.h.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,6 +16,7 @@
 
 #include "../../include/stfwi.h"
 #include "kernels.cuh"
+#include "kernels_tma.cuh"
 
 using namespace stfwi;
 
@@ -47,7 +50,15 @@ struct stfwi_handle {
     float *B = nullptr, *L2M = nullptr, *L = nullptr, *M = nullptr, *Lr = nullptr;
     float *bx = nullptr, *ax = nullptr, *ikx = nullptr, *bz = nullptr, *az = nullptr, *ikz = nullptr;
     float *vpmax = nullptr;
+    float *MATS = nullptr;  // [4][nz][P]: B, L2M, L, M
     bool model_set = false;
+    // TMA-pipelined variant: tensor maps and per-kernel shot groups
+    int variant = 0, sms = 148;
+    CUtensorMap tmF3{}, tmF2{}, tmA3{}, tmA2{}, tmM4{}, tmB1{};
+    int grp[4] = {1, 1, 1, 1}, spgk[4] = {1, 1, 1, 1};
+    int acc_groups = 1, acc_used = 1;
+    int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
+    int occ[4] = {1, 1, 1, 1};  // resident blocks per SM of fwd_vel, fwd_str, adj_a, adj_b
 
     // shots / receivers
     int nshot = 0;
@@ -317,7 +328,7 @@ __global__ void k_misfit_reduce(int nshot, int nrec, const double *mis_trace, do
 // physical grid.  EXACT: M = rho Vs^2, L2M = rho Vp^2, L = L2M - 2M; the
 // free-surface ratio Lr = -L/L2M contributes on row 0.  IMAGING:
 // fwi/imaging.py:165-167.
-__global__ void k_finalize(Geo g, int groups, const double *acc, const double *accLr,
+__global__ void k_finalize(Geo g, int groups, int lr_rows, const double *acc, const double *accLr,
                            const float *L2M, const float *L, const float *vs, const float *vp,
                            const float *rho, int want_exact, int want_img, double *out_exact,
                            double *out_img)
@@ -334,7 +345,7 @@ __global__ void k_finalize(Geo g, int groups, const double *acc, const double *a
     if (want_exact) {
         if (g.fs && pi == 0) {
             double glr = 0;
-            for (int k = 0; k < groups; ++k) glr += accLr[(long long)k * g.nx_dom + pj];
+            for (int k = 0; k < lr_rows; ++k) glr += accLr[(long long)k * g.nx_dom + pj];
             const long long o = (long long)(pi + g.z0) * g.P + pj + g.pad;
             const double l2m = L2M[o], l = L[o];
             gL += -glr / l2m;
@@ -373,7 +384,7 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
 }
 
 template <int FD>
-void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void launch_fwd_step_plain(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
     // one shot per block: the forward carries no cross-shot state (the
     // illumination sum uses FP64 atomics per cell and shot)
@@ -388,7 +399,24 @@ void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 }
 
 template <int FD>
-void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+{
+    if (h->variant == 1) return launch_fwd_step_plain<FD>(h, n, o, st);
+    using T = TileT<FD>;
+    const int tiles = h->g.tiles_x * h->g.tiles_z;
+    dim3 block(TX, NWARP);
+    prof_mark(h, 0, n, 0, st);
+    k_fwd_vel_t<FD><<<dim3(tiles, h->grp[0]), block, T::bytes(T::VEL, 3), st>>>(
+        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->status, h->tmF3, h->tmM4);
+    prof_mark(h, 0, n, 1, st);
+    prof_mark(h, 1, n, 0, st);
+    k_fwd_str_t<FD><<<dim3(tiles, h->grp[1]), block, T::bytes(T::STR, 2), st>>>(
+        h->g, mat_of(h), shots_of(h), recv_of(h), h->F, h->PX, h->PZ, n, h->spgk[1], o, h->tmF2);
+    prof_mark(h, 1, n, 1, st);
+}
+
+template <int FD>
+void launch_adj_step_plain(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
 {
     // U_a/V_a phase: one shot per block (no cross-shot state); strain phase:
     // shot groups, so the FP64 gradient sum over shots stays in registers
@@ -414,6 +442,30 @@ void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, 
 
 
 
+template <int FD>
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+{
+    if (h->variant == 1) return launch_adj_step_plain<FD>(h, n, ai, ao, st);
+    using T = TileT<FD>;
+    const int tiles = h->g.tiles_x * h->g.tiles_z;
+    dim3 block(TX, NWARP);
+    prof_mark(h, 2, n, 0, st);
+    k_adj_a_t<FD><<<dim3(tiles, h->grp[2]), block, T::bytes(T::ADA, 2), st>>>(
+        h->g, mat_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[2], ai, h->status, h->tmA3);
+    prof_mark(h, 2, n, 1, st);
+    prof_mark(h, 3, n, 0, st);
+    auto launch = [&](auto kern) {
+        kern<<<dim3(tiles, h->grp[3]), block, T::bytes(T::ADB, 3), st>>>(
+            h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[3], ao, h->status, h->tmA2,
+            h->tmB1);
+    };
+    if (ao.want_exact && ao.want_img) launch(k_adj_b_t<FD, true, true>);
+    else if (ao.want_exact) launch(k_adj_b_t<FD, true, false>);
+    else if (ao.want_img) launch(k_adj_b_t<FD, false, true>);
+    else launch(k_adj_b_t<FD, false, false>);
+    prof_mark(h, 3, n, 1, st);
+}
+
 stfwi_status zero_forward_state(stfwi_handle *h, cudaStream_t st)
 {
     const Geo &g = h->g;
@@ -438,8 +490,8 @@ stfwi_status zero_adjoint_state(stfwi_handle *h, cudaStream_t st)
         CK(h, cudaMemsetAsync(h->PZ + ((long long)s * NPZ + PZ_NFWD) * g.zstride, 0,
                               (size_t)2 * PZA_N * g.zstride * sizeof(float), st));
     }
-    CK(h, cudaMemsetAsync(h->acc, 0, (size_t)h->groups * 5 * g.nd * sizeof(double), st));
-    CK(h, cudaMemsetAsync(h->accLr, 0, (size_t)h->groups * g.nx_dom * sizeof(double), st));
+    CK(h, cudaMemsetAsync(h->acc, 0, (size_t)h->acc_used * 5 * g.nd * sizeof(double), st));
+    CK(h, cudaMemsetAsync(h->accLr, 0, (size_t)h->lr_used * g.nx_dom * sizeof(double), st));
     return STFWI_OK;
 }
 
@@ -521,6 +573,77 @@ void prof_accumulate(stfwi_handle *h, int k)
     cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- TMA set-up
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// row-major float32 array of `rank` dims (x fastest), box of `box` elements
+stfwi_status encode(stfwi_handle *h, CUtensorMap *m, void *base, int rank, const cuuint64_t *dims,
+                    const cuuint64_t *strides_bytes, const cuuint32_t *box)
+{
+    auto fn = encode_fn();
+    if (!fn) return fail(h, STFWI_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base, dims, strides_bytes, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(h, STFWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return STFWI_OK;
+}
+
+template <int FD>
+stfwi_status setup_tma_kernels(stfwi_handle *h)
+{
+    using T = TileT<FD>;
+    const void *kern[4] = {(const void *)k_fwd_vel_t<FD>, (const void *)k_fwd_str_t<FD>,
+                           (const void *)k_adj_a_t<FD>, (const void *)k_adj_b_t<FD, true, false>};
+    const size_t bytes[4] = {T::bytes(T::VEL, 3), T::bytes(T::STR, 2), T::bytes(T::ADA, 2), T::bytes(T::ADB, 3)};
+    const void *others[3] = {(const void *)k_adj_b_t<FD, true, true>, (const void *)k_adj_b_t<FD, false, true>,
+                             (const void *)k_adj_b_t<FD, false, false>};
+    for (int k = 0; k < 4; ++k) {
+        CK(h, cudaFuncSetAttribute(kern[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]));
+        CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[k], kern[k], NTHR, bytes[k]));
+        h->occ[k] = std::max(1, h->occ[k]);
+    }
+    for (const void *k : others)
+        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[3]));
+    return STFWI_OK;
+}
+
+stfwi_status setup_tensor_maps(stfwi_handle *h)
+{
+    const Geo &g = h->g;
+    const int H = h->d.fd_order / 2;
+    const cuuint64_t S = (cuuint64_t)h->d.max_shots;
+    const cuuint64_t fdims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)F_N, S};
+    const cuuint64_t fstr[3] = {(cuuint64_t)g.P * 4, (cuuint64_t)g.nz * g.P * 4, (cuuint64_t)F_N * g.nz * g.P * 4};
+    const cuuint32_t box3[4] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 3, 1};
+    const cuuint32_t box2[4] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 2, 1};
+    stfwi_status r;
+    if ((r = encode(h, &h->tmF3, h->F, 4, fdims, fstr, box3))) return r;
+    if ((r = encode(h, &h->tmF2, h->F, 4, fdims, fstr, box2))) return r;
+    if ((r = encode(h, &h->tmA3, h->A, 4, fdims, fstr, box3))) return r;
+    if ((r = encode(h, &h->tmA2, h->A, 4, fdims, fstr, box2))) return r;
+    const cuuint64_t mdims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, 4};
+    const cuuint64_t mstr[2] = {(cuuint64_t)g.P * 4, (cuuint64_t)g.nz * g.P * 4};
+    const cuuint32_t mbox4[3] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 4};
+    const cuuint32_t mbox1[3] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 1};
+    if ((r = encode(h, &h->tmM4, h->MATS, 3, mdims, mstr, mbox4))) return r;
+    if ((r = encode(h, &h->tmB1, h->MATS, 3, mdims, mstr, mbox1))) return r;
+    return STFWI_OK;
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -580,6 +703,22 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
     h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
     h->spg = (d->max_shots + h->groups - 1) / h->groups;
+    h->variant = d->kernel_variant == 1 ? 1 : 0;
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (h->variant == 0) {
+        stfwi_status r = STFWI_OK;
+        switch (d->fd_order) {
+        case 2: r = setup_tma_kernels<2>(h); break;
+        case 4: r = setup_tma_kernels<4>(h); break;
+        default: r = setup_tma_kernels<8>(h); break;
+        }
+        if (r) { delete h; return r; }
+        const int spg0 = d->shot_group > 0 ? d->shot_group : 2;
+        h->acc_groups = std::max(1, (d->max_shots + spg0 - 1) / spg0);
+    } else {
+        h->acc_groups = h->groups;
+    }
+    h->acc_used = h->acc_groups;
     h->slots = d->nt;
 
     auto alloc = [&](void **ptr, size_t bytes) -> bool {
@@ -592,8 +731,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     const long long nrec = std::max(d->nrec, 1);
     bool ok = true;
     ok &= alloc((void **)&h->vs, nd * 4) && alloc((void **)&h->vp, nd * 4) && alloc((void **)&h->rho, nd * 4);
-    ok &= alloc((void **)&h->B, NP * 4) && alloc((void **)&h->L2M, NP * 4) && alloc((void **)&h->L, NP * 4) &&
-          alloc((void **)&h->M, NP * 4) && alloc((void **)&h->Lr, p.P * 4);
+    ok &= alloc((void **)&h->MATS, 4 * NP * 4) && alloc((void **)&h->Lr, p.P * 4);
+    if (ok) { h->B = h->MATS; h->L2M = h->MATS + NP; h->L = h->MATS + 2 * NP; h->M = h->MATS + 3 * NP; }
     ok &= alloc((void **)&h->bx, p.P * 4) && alloc((void **)&h->ax, p.P * 4) && alloc((void **)&h->ikx, p.P * 4);
     ok &= alloc((void **)&h->bz, p.nz * 4) && alloc((void **)&h->az, p.nz * 4) && alloc((void **)&h->ikz, p.nz * 4);
     ok &= alloc((void **)&h->vpmax, 16) && alloc((void **)&h->status, 16);
@@ -609,8 +748,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
           alloc((void **)&h->rec_adj, (size_t)S * 4 * d->nt * nrec * 4) &&
           alloc((void **)&h->obs, (size_t)S * d->nt * nrec * 4);
     ok &= alloc((void **)&h->snap, p.snap) && alloc((void **)&h->row0, p.row0);
-    ok &= alloc((void **)&h->acc, (size_t)h->groups * 5 * nd * 8) &&
-          alloc((void **)&h->accLr, (size_t)h->groups * std::max(d->nx_dom, 1) * 8) &&
+    ok &= alloc((void **)&h->acc, (size_t)h->acc_groups * 5 * nd * 8) &&
+          alloc((void **)&h->accLr, (size_t)std::max(h->acc_groups, d->max_shots) * std::max(d->nx_dom, 1) * 8) &&
           alloc((void **)&h->gtmp, (size_t)6 * nd * 8);
     ok &= alloc((void **)&h->energy, (size_t)p.nz * p.nx * 8);
     ok &= alloc((void **)&h->mis_trace, (size_t)S * nrec * 8) && alloc((void **)&h->mis_shot, (size_t)S * 8);
@@ -627,6 +766,18 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_CUDA;
     }
     cudaMemset(h->status, 0, 16);
+    // pitch padding and never-written cells read as zero by the tile copies
+    cudaMemset(h->MATS, 0, (size_t)4 * NP * 4);
+    cudaMemset(h->F, 0, (size_t)S * F_N * NP * 4);
+    cudaMemset(h->A, 0, (size_t)S * F_N * NP * 4);
+    if (h->variant == 0) {
+        stfwi_status r = setup_tensor_maps(h);
+        if (r) {
+            fprintf(stderr, "stfwi_create: %s\n", h->err.c_str());
+            stfwi_destroy(h);
+            return r;
+        }
+    }
     *out = h;
     return STFWI_OK;
 }
@@ -636,7 +787,7 @@ void stfwi_destroy(stfwi_handle *h)
     if (!h) return;
     if (h->hs) cudaStreamSynchronize(h->hs);
     drop_graphs(h);
-    void *bufs[] = {h->vs, h->vp, h->rho, h->B, h->L2M, h->L, h->M, h->Lr, h->bx, h->ax, h->ikx, h->bz,
+    void *bufs[] = {h->vs, h->vp, h->rho, h->MATS, h->Lr, h->bx, h->ax, h->ikx, h->bz,
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
                     h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
@@ -734,6 +885,23 @@ stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
     h->nshot = nshot;
     g.nshot = nshot;
     h->spg = std::max(1, (nshot + h->groups - 1) / h->groups);
+    if (h->variant == 0) {
+        const int tiles = g.tiles_x * g.tiles_z;
+        for (int k = 0; k < 4; ++k) {
+            // two shots per block by default: enough blocks to keep every SM
+            // busy, and a second copy in flight while the first computes
+            const int spg = h->d.shot_group > 0 ? h->d.shot_group : 2;
+            int G = (nshot + spg - 1) / spg;
+            if (k == 3) G = std::min(G, h->acc_groups);
+            h->spgk[k] = (nshot + G - 1) / G;
+            h->grp[k] = (nshot + h->spgk[k] - 1) / h->spgk[k];
+        }
+        h->acc_used = h->grp[3];
+        h->lr_used = h->grp[2];
+    } else {
+        h->acc_used = h->groups;
+        h->lr_used = nshot;  // the plain U_a/V_a phase runs one shot per block row
+    }
     h->shots_set = true;
     h->stored = false;
     if (h->model_set) {
@@ -860,7 +1028,7 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
             }
         }
         if (ex || im)
-            k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->groups, h->acc, h->accLr, h->L2M,
+            k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->acc_used, h->lr_used, h->acc, h->accLr, h->L2M,
                                                                       h->L, h->vs, h->vp, h->rho, ex, im,
                                                                       h->gtmp, h->gtmp + 3 * g.nd);
         CK(h, cudaGetLastError());
@@ -939,6 +1107,7 @@ stfwi_status stfwi_check(stfwi_handle *h, void *stream)
     CK(h, cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(h, cudaStreamSynchronize((cudaStream_t)stream));
     if (v & 1) return fail(h, STFWI_ERR_NONFINITE, "a receiver sample became non-finite (unstable dt or model?)");
+    if (v & ST_TIMEOUT) return fail(h, STFWI_ERR_TIMEOUT, "a tile copy did not complete within the wait limit");
     return STFWI_OK;
 }
 

@@ -45,14 +45,15 @@ class Solver:
     forward_jax / build_forward_fn (fwi/forward.py:119-123, :508-509)."""
 
     def __init__(self, nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, max_shots, fd_order=2,
-                 free_surface=True, want_gradient=True, shot_group=0, mem_budget_gb=0.0):
+                 free_surface=True, want_gradient=True, shot_group=0, mem_budget_gb=0.0,
+                 kernel_variant=0):
         if fd_order not in (2, 4, 8):
             raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
         self.lib = N.load()
         self.desc = N.StfwiDesc(int(nz_dom), int(nx_dom), int(pad), int(fd_order),
                                 int(bool(free_surface)), int(nt), int(nrec), int(max_shots),
                                 float(dx), float(dz), float(dt), float(fc), int(bool(want_gradient)),
-                                int(shot_group), float(mem_budget_gb))
+                                int(shot_group), float(mem_budget_gb), int(kernel_variant), 0)
         h = ct.c_void_p()
         st = self.lib.stfwi_create(ct.byref(self.desc), ct.byref(h))
         if st != N.STFWI_OK:
@@ -76,7 +77,8 @@ class Solver:
         d = N.StfwiDesc(kw["nz_dom"], kw["nx_dom"], kw["pad"], kw.get("fd_order", 2),
                         int(kw.get("free_surface", True)), kw["nt"], kw["nrec"], kw["max_shots"],
                         kw["dx"], kw["dz"], kw["dt"], kw["fc"], int(kw.get("want_gradient", True)),
-                        kw.get("shot_group", 0), kw.get("mem_budget_gb", 0.0))
+                        kw.get("shot_group", 0), kw.get("mem_budget_gb", 0.0),
+                        kw.get("kernel_variant", 0), 0)
         return int(lib.stfwi_workspace_bytes(ct.byref(d)))
 
     # ------------------------------------------------------------------ helpers

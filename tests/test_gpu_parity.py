@@ -28,15 +28,19 @@ def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx
                   want_gradient=want_gradient, **kw)
 
 
+VARIANTS = [0, 1]  # TMA-pipelined tiles, plain shared-memory tiles
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("fd,fs,st", C.CONFIGS)
-def test_forward_and_adjoint_vs_oracle(fd, fs, st):
+def test_forward_and_adjoint_vs_oracle(fd, fs, st, variant):
     """The reference's dot-product case (test_adjoint_kernel.py) on the GPU:
     seismograms and the source adjoint against the FP64 oracle, and the
     dot-product identity of the FP32 kernels."""
     vs, vp, rho = C.model()
     sx, sz, rx, rz = C.acquisition(fs, st)
     s_in, ys = C.random_vectors()
-    S = _solver(C.NT, len(rx), 1, fd, fs)
+    S = _solver(C.NT, len(rx), 1, fd, fs, kernel_variant=variant)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots([sx], [sz], [st], s_in.astype(np.float32))
@@ -57,9 +61,10 @@ def test_forward_and_adjoint_vs_oracle(fd, fs, st):
     S.close()
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("fd,fs,st", [(8, True, "force"), (8, True, "moment"), (4, False, "force"),
                                       (2, False, "moment")])
-def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st):
+def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st, variant):
     """Model gradients of the GPU (FP32 stencils, FP64 sums) against the
     FP64 oracle on a small case: exact (AD) and imaging formula."""
     vs, vp, rho = C.model()
@@ -73,7 +78,7 @@ def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st):
               scale=1.0, invert="vs_vp", **geo)
     (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
     (gi_vs, gi_vp, _), _ = O.compute_gradient("adjoint", Vs=vs, Vp=vp, rho=rho, **kw)
-    S = _solver(nt, len(rx), 1, fd, fs, want_gradient=True)
+    S = _solver(nt, len(rx), 1, fd, fs, want_gradient=True, kernel_variant=variant)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots([sx], [sz], [st], wav.astype(np.float32))
@@ -123,3 +128,43 @@ def test_marmousi_known_answers(known_answers):
           f"g_Vs_HC rel-L2 {e_hc:.3e}")
     assert e_ad < 1e-3 and e_hc < 1e-3, (e_ad, e_hc)
     S.close()
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_batch_of_shots_matches_single_shots(variant):
+    """A batch of 7 mixed force/moment shots (several shots per block, both
+    pipeline stages in use) gives each shot's traces and the summed gradient
+    of the single-shot runs."""
+    vs, vp, rho = C.model()
+    nt, fd, fs = 90, 8, True
+    rx = np.arange(1, C.NX - 1, 3, dtype=np.int32)
+    rz = np.ones_like(rx)
+    sx = np.array([3, 7, 11, 15, 19, 23, 27])
+    sz = np.array([2, 5, 3, 6, 2, 4, 3])
+    types = ["force", "moment"] * 3 + ["force"]
+    wav = (O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9).astype(np.float32)
+    rng = np.random.default_rng(5)
+    obs = rng.standard_normal((7, nt, len(rx))).astype(np.float32) * 1e-9
+    S = _solver(nt, len(rx), 7, fd, fs, want_gradient=True, kernel_variant=variant, shot_group=2)
+    S.set_model(vs, vp, rho)
+    S.set_receivers(rx, rz)
+    S.set_shots(sx, sz, types, wav)
+    S.forward(store=True)
+    rec = S.records()
+    mis = S.misfit(obs, 1, 1.0)
+    g = S.gradient(exact=True)["exact"][0]
+    S.close()
+    gsum = np.zeros_like(g)
+    for k in range(7):
+        S1 = _solver(nt, len(rx), 1, fd, fs, want_gradient=True, kernel_variant=1)
+        S1.set_model(vs, vp, rho)
+        S1.set_receivers(rx, rz)
+        S1.set_shots(sx[k:k + 1], sz[k:k + 1], types[k:k + 1], wav)
+        S1.forward(store=True)
+        r1 = S1.records()[0]
+        assert _rel(rec[k], r1) < 1e-6, (k, _rel(rec[k], r1))
+        m1 = S1.misfit(obs[k:k + 1], 1, 1.0, nshot_norm=7)
+        assert abs(m1[0] / mis[k] - 1) < 1e-6
+        gsum += S1.gradient(exact=True)["exact"][0]
+        S1.close()
+    assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
