@@ -53,6 +53,7 @@ struct Geo {
     int tiles_x, tiles_z;
     float dtdx, dtdz, dzdx, dt;
     float inv2dx, inv2dz;      // 1/(2 dx), 1/(2 dz) (imaging condition)
+    float dtdxdz;              // dt / (dx dz) (force source)
     long long fstride;         // nz*P
     long long xstride;         // nz*xs_n  (one x-psi array)
     long long zstride;         // zs_n*P   (one z-psi array)

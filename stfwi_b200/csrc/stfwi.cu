@@ -16,7 +16,7 @@
 
 #include "../../include/stfwi.h"
 #include "kernels.cuh"
-#include "kernels_tma.cuh"
+#include "kernels_v3.cuh"
 
 using namespace stfwi;
 
@@ -54,7 +54,9 @@ struct stfwi_handle {
     bool model_set = false;
     // TMA-pipelined variant: tensor maps and per-kernel shot groups
     int variant = 0, sms = 148;
-    CUtensorMap tmF3{}, tmF2{}, tmA3{}, tmA2{}, tmM4{}, tmB1{};
+    CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
+    int tx3 = 1, tz64 = 1, tz32 = 1;                 // tile counts of the 64- and 32-row tilings
+    int *tile_start64 = nullptr, *tile_rec64 = nullptr;  // receivers grouped by 64-row tiles
     int grp[4] = {1, 1, 1, 1}, spgk[4] = {1, 1, 1, 1};
     int acc_groups = 1, acc_used = 1;
     int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
@@ -402,16 +404,16 @@ template <int FD>
 void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
     if (h->variant == 1) return launch_fwd_step_plain<FD>(h, n, o, st);
-    using T = TileT<FD>;
-    const int tiles = h->g.tiles_x * h->g.tiles_z;
+    const int tiles = h->tx3 * h->tz64;
     dim3 block(TX, NWARP);
+    Recv rv64{h->tile_start64, h->tile_rec64, h->rx, h->rz};
     prof_mark(h, 0, n, 0, st);
-    k_fwd_vel_t<FD><<<dim3(tiles, h->grp[0]), block, T::bytes(T::VEL, 3), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->status, h->tmF3, h->tmM4);
+    k3_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L3<FD>::bytes(L3<FD>::VEL, 2), st>>>(
+        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->tx3, h->status, h->tmS);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
-    k_fwd_str_t<FD><<<dim3(tiles, h->grp[1]), block, T::bytes(T::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), recv_of(h), h->F, h->PX, h->PZ, n, h->spgk[1], o, h->tmF2);
+    k3_fwd_str<FD><<<dim3(tiles, h->grp[1]), block, L3<FD>::bytes(L3<FD>::STR, 2), st>>>(
+        h->g, mat_of(h), shots_of(h), rv64, h->F, h->PX, h->PZ, n, h->spgk[1], h->tx3, o, h->tmV);
     prof_mark(h, 1, n, 1, st);
 }
 
@@ -446,23 +448,22 @@ template <int FD>
 void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
 {
     if (h->variant == 1) return launch_adj_step_plain<FD>(h, n, ai, ao, st);
-    using T = TileT<FD>;
-    const int tiles = h->g.tiles_x * h->g.tiles_z;
     dim3 block(TX, NWARP);
+    Recv rv64{h->tile_start64, h->tile_rec64, h->rx, h->rz};
     prof_mark(h, 2, n, 0, st);
-    k_adj_a_t<FD><<<dim3(tiles, h->grp[2]), block, T::bytes(T::ADA, 2), st>>>(
-        h->g, mat_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[2], ai, h->status, h->tmA3);
+    k3_adj_a<FD><<<dim3(h->tx3 * h->tz64, h->grp[2]), block, L3<FD>::bytes(L3<FD>::ADA, 2), st>>>(
+        h->g, mat_of(h), rv64, h->A, h->PX, h->PZ, n, h->spgk[2], h->tx3, ai, h->status, h->tmE);
     prof_mark(h, 2, n, 1, st);
     prof_mark(h, 3, n, 0, st);
     auto launch = [&](auto kern) {
-        kern<<<dim3(tiles, h->grp[3]), block, T::bytes(T::ADB, 3), st>>>(
-            h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[3], ao, h->status, h->tmA2,
-            h->tmB1);
+        kern<<<dim3(h->tx3 * h->tz32, h->grp[3]), block, L3<FD>::bytes(L3<FD>::ADB, 2), st>>>(
+            h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[3], h->tx3, ao, h->status,
+            h->tmPQ);
     };
-    if (ao.want_exact && ao.want_img) launch(k_adj_b_t<FD, true, true>);
-    else if (ao.want_exact) launch(k_adj_b_t<FD, true, false>);
-    else if (ao.want_img) launch(k_adj_b_t<FD, false, true>);
-    else launch(k_adj_b_t<FD, false, false>);
+    if (ao.want_exact && ao.want_img) launch(k3_adj_b<FD, true, true>);
+    else if (ao.want_exact) launch(k3_adj_b<FD, true, false>);
+    else if (ao.want_img) launch(k3_adj_b<FD, false, true>);
+    else launch(k3_adj_b<FD, false, false>);
     prof_mark(h, 3, n, 1, st);
 }
 
@@ -605,19 +606,19 @@ stfwi_status encode(stfwi_handle *h, CUtensorMap *m, void *base, int rank, const
 template <int FD>
 stfwi_status setup_tma_kernels(stfwi_handle *h)
 {
-    using T = TileT<FD>;
-    const void *kern[4] = {(const void *)k_fwd_vel_t<FD>, (const void *)k_fwd_str_t<FD>,
-                           (const void *)k_adj_a_t<FD>, (const void *)k_adj_b_t<FD, true, false>};
-    const size_t bytes[4] = {T::bytes(T::VEL, 3), T::bytes(T::STR, 2), T::bytes(T::ADA, 2), T::bytes(T::ADB, 3)};
-    const void *others[3] = {(const void *)k_adj_b_t<FD, true, true>, (const void *)k_adj_b_t<FD, false, true>,
-                             (const void *)k_adj_b_t<FD, false, false>};
-    for (int k = 0; k < 4; ++k) {
+    using Lk = L3<FD>;
+    const void *kern[] = {(const void *)k3_fwd_vel<FD>, (const void *)k3_fwd_str<FD>, (const void *)k3_adj_a<FD>,
+                          (const void *)k3_adj_b<FD, true, false>, (const void *)k3_adj_b<FD, true, true>,
+                          (const void *)k3_adj_b<FD, false, true>, (const void *)k3_adj_b<FD, false, false>};
+    const size_t bytes[] = {Lk::bytes(Lk::VEL, 2), Lk::bytes(Lk::STR, 2), Lk::bytes(Lk::ADA, 2), Lk::bytes(Lk::ADB, 2),
+                            Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2)};
+    for (int k = 0; k < 7; ++k) {
         CK(h, cudaFuncSetAttribute(kern[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]));
-        CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[k], kern[k], NTHR, bytes[k]));
-        h->occ[k] = std::max(1, h->occ[k]);
+        if (k < 4) {
+            CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[k], kern[k], NTHR, bytes[k]));
+            h->occ[k] = std::max(1, h->occ[k]);
+        }
     }
-    for (const void *k : others)
-        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[3]));
     return STFWI_OK;
 }
 
@@ -628,19 +629,14 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
     const cuuint64_t S = (cuuint64_t)h->d.max_shots;
     const cuuint64_t fdims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)F_N, S};
     const cuuint64_t fstr[3] = {(cuuint64_t)g.P * 4, (cuuint64_t)g.nz * g.P * 4, (cuuint64_t)F_N * g.nz * g.P * 4};
-    const cuuint32_t box3[4] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 3, 1};
-    const cuuint32_t box2[4] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 2, 1};
+    const cuuint32_t box3[4] = {(cuuint32_t)SW3, (cuuint32_t)(RPT3 * NWARP + 2 * H), 3, 1};
+    const cuuint32_t box2[4] = {(cuuint32_t)SW3, (cuuint32_t)(RPT3 * NWARP + 2 * H), 2, 1};
+    const cuuint32_t box2s[4] = {(cuuint32_t)SW3, (cuuint32_t)(4 * NWARP + 2 * H), 2, 1};
     stfwi_status r;
-    if ((r = encode(h, &h->tmF3, h->F, 4, fdims, fstr, box3))) return r;
-    if ((r = encode(h, &h->tmF2, h->F, 4, fdims, fstr, box2))) return r;
-    if ((r = encode(h, &h->tmA3, h->A, 4, fdims, fstr, box3))) return r;
-    if ((r = encode(h, &h->tmA2, h->A, 4, fdims, fstr, box2))) return r;
-    const cuuint64_t mdims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, 4};
-    const cuuint64_t mstr[2] = {(cuuint64_t)g.P * 4, (cuuint64_t)g.nz * g.P * 4};
-    const cuuint32_t mbox4[3] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 4};
-    const cuuint32_t mbox1[3] = {(cuuint32_t)SWT, (cuuint32_t)(TZ + 2 * H), 1};
-    if ((r = encode(h, &h->tmM4, h->MATS, 3, mdims, mstr, mbox4))) return r;
-    if ((r = encode(h, &h->tmB1, h->MATS, 3, mdims, mstr, mbox1))) return r;
+    if ((r = encode(h, &h->tmS, h->F, 4, fdims, fstr, box3))) return r;
+    if ((r = encode(h, &h->tmV, h->F, 4, fdims, fstr, box2))) return r;
+    if ((r = encode(h, &h->tmE, h->A, 4, fdims, fstr, box3))) return r;
+    if ((r = encode(h, &h->tmPQ, h->A, 4, fdims, fstr, box2s))) return r;
     return STFWI_OK;
 }
 
@@ -700,10 +696,14 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.dtdx = (float)(d->dt / d->dx); g.dtdz = (float)(d->dt / d->dz); g.dzdx = (float)(d->dz / d->dx);
     g.dt = (float)d->dt;
     g.inv2dx = (float)(1.0 / (2.0 * d->dx)); g.inv2dz = (float)(1.0 / (2.0 * d->dz));
+    g.dtdxdz = (float)(d->dt / (d->dx * d->dz));
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
     h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
     h->spg = (d->max_shots + h->groups - 1) / h->groups;
     h->variant = d->kernel_variant == 1 ? 1 : 0;
+    h->tx3 = (int)((p.nx + TX - 1) / TX);
+    h->tz64 = (int)((p.nz + RPT3 * NWARP - 1) / (RPT3 * NWARP));
+    h->tz32 = (int)((p.nz + 4 * NWARP - 1) / (4 * NWARP));
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
     if (h->variant == 0) {
         stfwi_status r = STFWI_OK;
@@ -739,6 +739,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     ok &= alloc((void **)&h->sx, S * 4) && alloc((void **)&h->sz, S * 4) && alloc((void **)&h->stype, S * 4);
     ok &= alloc((void **)&h->wav, S * d->nt * 4) && alloc((void **)&h->fcoef, S * 4) &&
           alloc((void **)&h->mcoef, S * 4) && alloc((void **)&h->lm, S * 4);
+    ok &= alloc((void **)&h->tile_start64, ((size_t)h->tx3 * h->tz64 + 1) * 4) &&
+          alloc((void **)&h->tile_rec64, nrec * 4);
     ok &= alloc((void **)&h->tile_start, ((size_t)p.tiles_x * p.tiles_z + 1) * 4) &&
           alloc((void **)&h->tile_rec, nrec * 4) && alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
     ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
@@ -791,7 +793,7 @@ void stfwi_destroy(stfwi_handle *h)
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
                     h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
-                    h->mis_trace, h->mis_shot, h->src_a};
+                    h->mis_trace, h->mis_shot, h->src_a, h->tile_start64, h->tile_rec64};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (int k = 0; k < 4; ++k)
@@ -854,6 +856,16 @@ stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *r
     CK(h, cudaMemcpy(h->rz, rz.data(), rz.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile_rec, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
+    {   // the same grouping for the 64-row tiles
+        const int nt64 = h->tx3 * h->tz64, TZ64 = RPT3 * NWARP;
+        std::vector<int> c64(nt64 + 1, 0), s64(nt64 + 1, 0), l64(std::max(nrec, 1));
+        for (int r = 0; r < nrec; ++r) c64[(rz[r] / TZ64) * h->tx3 + rx[r] / TX]++;
+        for (int t = 0; t < nt64; ++t) s64[t + 1] = s64[t] + c64[t];
+        std::vector<int> f64(s64.begin(), s64.end() - 1);
+        for (int r = 0; r < nrec; ++r) l64[f64[(rz[r] / TZ64) * h->tx3 + rx[r] / TX]++] = r;
+        CK(h, cudaMemcpy(h->tile_start64, s64.data(), s64.size() * 4, cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(h->tile_rec64, l64.data(), l64.size() * 4, cudaMemcpyHostToDevice));
+    }
     h->recv_set = true;
     return STFWI_OK;
 }
@@ -1107,7 +1119,7 @@ stfwi_status stfwi_check(stfwi_handle *h, void *stream)
     CK(h, cudaMemcpyAsync(&v, h->status, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(h, cudaStreamSynchronize((cudaStream_t)stream));
     if (v & 1) return fail(h, STFWI_ERR_NONFINITE, "a receiver sample became non-finite (unstable dt or model?)");
-    if (v & ST_TIMEOUT) return fail(h, STFWI_ERR_TIMEOUT, "a tile copy did not complete within the wait limit");
+    if (v & ST_TIMEOUT3) return fail(h, STFWI_ERR_TIMEOUT, "a tile copy did not complete within the wait limit");
     return STFWI_OK;
 }
 
