@@ -149,6 +149,23 @@ stfwi_status stfwi_profile(stfwi_handle *h, int32_t every);
  * Synchronises the handle's stream; resets the sums. */
 stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out);
 
+/* Residual preparation that allocates nothing (no counterpart in the
+ * reference): the same misfit and adjoint sources as stfwi_misfit, without a
+ * handle, for callers that cannot call cudaMalloc -- e.g. a custom call made
+ * from inside a framework that has reserved most of device memory for its own
+ * pool, or code recording a stream capture.  All pointers are device memory:
+ * pred [nshot][4][nt][nrec] (the layout stfwi_get_records returns), obs
+ * [nshot][nt][nrec], rec_adj [nshot][4][nt][nrec] (written), misfit_out
+ * [nshot] FP64 (written).  Its only scratch is a fixed device array of
+ * 262144 FP64 per-trace sums (2 MiB, held by every GPU that loads the library
+ * until exit): nshot * nrec above that limit returns STFWI_ERR_INVALID.  The
+ * first call on a device looks the array up (cudaGetSymbolAddress) and should
+ * come before any stream capture on that device.  Calls share the array, so
+ * calls that overlap on the GPU race.  Errors are printed to stderr. */
+stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t nrec, const float *pred,
+                                  const float *obs, const stfwi_misfit_desc *m, float *rec_adj,
+                                  double *misfit_out, void *stream);
+
 /* Padded-grid shape of a descriptor. */
 void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t);
 

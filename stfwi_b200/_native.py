@@ -25,8 +25,10 @@ EXPORTS = (
     "stfwi_workspace_bytes", "stfwi_create", "stfwi_destroy", "stfwi_last_error", "stfwi_set_model",
     "stfwi_set_receivers", "stfwi_set_shots", "stfwi_forward", "stfwi_get_records", "stfwi_misfit",
     "stfwi_set_adjoint_sources", "stfwi_gradient", "stfwi_illumination", "stfwi_check",
-    "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times",
+    "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
 )
+
+NOALLOC_MAX_TRACES = 1 << 18
 
 
 class StfwiDesc(ct.Structure):
@@ -86,5 +88,6 @@ def load():
         L.stfwi_grid_shape.restype = None
         L.stfwi_profile.argtypes = [H, i32]
         L.stfwi_kernel_times.argtypes = [H, vp]
+        L.stfwi_misfit_noalloc.argtypes = [i32, i32, i32, vp, vp, ct.POINTER(StfwiMisfitDesc), vp, vp, vp]
         _lib = L
     return _lib

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1124,3 +1125,84 @@ stfwi_status stfwi_check(stfwi_handle *h, void *stream)
 }
 
 }  // extern "C"
+
+// ================================================================ no-allocation misfit
+
+// Residual preparation without any allocation, for callers that must not
+// call cudaMalloc: an XLA custom call running inside a framework that has
+// already reserved most of the device memory for its own pool (the JAX
+// drivers of this workload run with 90 % preallocated), or code recording
+// into a stream capture.  The only scratch it needs, one FP64 partial sum
+// per trace, lives in this file-scope device array; every GPU that loads the
+// library holds it until the process exits.
+static constexpr int STFWI_NOALLOC_MAX_TRACES = 1 << 18;  // nshot * nrec <= 262144 (2 MiB)
+static __device__ __align__(256) double g_noalloc_trace_sums[STFWI_NOALLOC_MAX_TRACES];
+
+namespace {
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[256] = {nullptr};
+}  // namespace
+
+extern "C" stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t nrec, const float *pred,
+                                             const float *obs, const stfwi_misfit_desc *m, float *rec_adj,
+                                             double *misfit_out, void *stream)
+{
+    if (!pred || !obs || !m || !rec_adj || !misfit_out || nshot < 1 || nt < 1 || nrec < 1) {
+        fprintf(stderr, "stfwi_misfit_noalloc: null pointer or empty size\n");
+        return STFWI_ERR_INVALID;
+    }
+    if ((long long)nshot * nrec > STFWI_NOALLOC_MAX_TRACES) {
+        fprintf(stderr, "stfwi_misfit_noalloc: %lld traces exceed the fixed scratch of %d traces\n",
+                (long long)nshot * nrec, STFWI_NOALLOC_MAX_TRACES);
+        return STFWI_ERR_INVALID;
+    }
+    if (m->component < 0 || m->component > 3 || m->nsos < 0 || m->nsos > MAX_SOS || (m->nsos > 0 && !m->sos)) {
+        fprintf(stderr, "stfwi_misfit_noalloc: bad component %d or nsos %d\n", m->component, m->nsos);
+        return STFWI_ERR_INVALID;
+    }
+    SosParams sp{};
+    sp.nsos = m->nsos;
+    for (int k = 0; k < m->nsos; ++k) {
+        const double *c = m->sos + 6 * k;
+        if (c[3] == 0.0) {
+            fprintf(stderr, "stfwi_misfit_noalloc: sos section %d has a0 = 0\n", k);
+            return STFWI_ERR_INVALID;
+        }
+        sp.c[k][0] = c[0] / c[3]; sp.c[k][1] = c[1] / c[3]; sp.c[k][2] = c[2] / c[3];
+        sp.c[k][3] = c[4] / c[3]; sp.c[k][4] = c[5] / c[3];
+    }
+    // device address of the scratch, looked up once per device with that
+    // device current (the host-side symbol is only a stand-in)
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return STFWI_ERR_CUDA;
+    double *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            cudaError_t e = cudaGetSymbolAddress((void **)&g_noalloc_ptr[dev], g_noalloc_trace_sums);
+            if (e != cudaSuccess) {
+                fprintf(stderr, "stfwi_misfit_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
+                g_noalloc_ptr[dev] = nullptr;
+                return STFWI_ERR_CUDA;
+            }
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    Geo g{};
+    g.nshot = nshot;
+    g.nt = nt;
+    g.nrec = nrec;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int ntap = std::min(std::max(m->n_taper, 0), nt);
+    const int nnorm = m->reserved > 0 ? m->reserved : nshot;
+    const int n = nshot * nrec, thr = 128;
+    k_misfit<<<(n + thr - 1) / thr, thr, 0, st>>>(g, m->component, ntap, sp, m->scale, nnorm, pred, obs, rec_adj,
+                                                 scratch);
+    k_misfit_reduce<<<(nshot + 127) / 128, 128, 0, st>>>(nshot, nrec, scratch, misfit_out);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "stfwi_misfit_noalloc: launch: %s\n", cudaGetErrorString(e));
+        return STFWI_ERR_CUDA;
+    }
+    return STFWI_OK;
+}

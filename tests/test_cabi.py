@@ -1,0 +1,67 @@
+"""The C ABI without a GPU: the library loads, exports every function that
+include/stfwi.h declares, and its host-only paths behave."""
+import ctypes as ct
+import os
+import re
+
+import pytest
+
+from tests.conftest import ROOT
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "stfwi.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(stfwi_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    names = _declared()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(N.EXPORTS), set(names) ^ set(N.EXPORTS)
+
+
+def test_workspace_and_grid_shape_are_host_only():
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    d = N.StfwiDesc(152, 500, 20, 8, 1, 2000, 250, 50, 20.0, 20.0, 1.5e-3, 5.0, 1, 0, 0.0, 0, 0)
+    nz, nx = ct.c_int32(), ct.c_int32()
+    lib.stfwi_grid_shape(ct.byref(d), ct.byref(nz), ct.byref(nx))
+    assert (nz.value, nx.value) == (172, 540)
+    ws = lib.stfwi_workspace_bytes(ct.byref(d))
+    # the strain history dominates: 50 shots x 2000 steps x 3 x 76000 cells x 4 B
+    assert 91e9 < ws < 95e9
+    d.want_gradient = 0
+    assert lib.stfwi_workspace_bytes(ct.byref(d)) < 2e9
+
+
+def test_create_rejects_bad_descriptors_before_touching_a_device():
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    h = ct.c_void_p()
+    d = N.StfwiDesc(24, 32, 8, 6, 1, 10, 3, 1, 10.0, 10.0, 1e-3, 15.0, 0, 0, 0.0, 0, 0)
+    assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_UNSUPPORTED
+    d.fd_order = 8
+    d.pad = 2  # thinner than the stencil half-width
+    assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
+    d.pad, d.dt = 8, -1.0
+    assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
+
+
+def test_noalloc_size_check_runs_on_the_host():
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    m = N.StfwiMisfitDesc(1, 0, 0, 0, 1.0, None)
+    dummy = ct.c_void_p(16)
+    st = lib.stfwi_misfit_noalloc(2, 10, N.NOALLOC_MAX_TRACES, dummy, dummy, ct.byref(m), dummy, dummy, None)
+    assert st == N.STFWI_ERR_INVALID
+
+
+def test_solver_rejects_unsupported_options_on_the_host():
+    from stfwi_b200 import Solver
+    with pytest.raises(NotImplementedError):
+        Solver(24, 32, 10.0, 10.0, 1e-3, 10, 15.0, 8, 3, 1, fd_order=6)
