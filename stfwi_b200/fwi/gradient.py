@@ -1,0 +1,93 @@
+"""compute_gradient with the reference's signature (fwi/gradient.py:48-99).
+
+Backends: ``'cuda'`` (alias ``'ad'``) returns the exact gradient of the
+discrete forward, what the reference's ``'ad'`` backend gets from JAX AD;
+``'cuda_imaging'`` (alias ``'adjoint'``) returns the reference's imaging
+condition (fwi/imaging.py), fused into the adjoint sweep.  The forward, the
+residual preparation (filter, taper, FP64 misfit) and the adjoint all run on
+the GPU; the post-processing (smoothing, source taper, illumination) is the
+reference's host arithmetic.  Unlike the reference's ``'adjoint'`` backend,
+whose forward always injects a force (fwi/gradient.py:176-180), the forward
+and the adjoint here use the same ``src_type``.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from ..solver import Solver
+from .loss import gaussian_smooth_2d
+
+_BACKENDS = {"cuda": "exact", "ad": "exact", "cuda_imaging": "imaging", "adjoint": "imaging"}
+_CACHE = {}
+
+
+def clear_cache():
+    """Release the GPU handles kept between calls."""
+    for S in _CACHE.values():
+        S.close()
+    _CACHE.clear()
+
+
+def _solver(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order, free_surface):
+    key = (nz_dom, nx_dom, float(dx), float(dz), float(dt), nt, float(fc), pad, nrec, nshot, fd_order,
+           bool(free_surface))
+    S = _CACHE.get(key)
+    if S is None:
+        if len(_CACHE) >= 4:
+            clear_cache()
+        S = Solver(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order=fd_order,
+                   free_surface=free_surface, want_gradient=True)
+        _CACHE[key] = S
+    return S
+
+
+def _postprocess(grads, grad_smooth_sigma, source_taper, illumination):
+    """fwi/gradient.py:266-277."""
+    out = list(grads)
+    if grad_smooth_sigma is not None:
+        out = [gaussian_smooth_2d(g, grad_smooth_sigma) for g in out]
+    if source_taper is not None:
+        st = np.asarray(source_taper)
+        out = [g * st for g in out]
+    if illumination is not None:
+        il = np.asarray(illumination)
+        out = [g * il for g in out]
+    return tuple(out)
+
+
+def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observed, rec_x, rec_z, nx_dom,
+                     nz_dom, dx, dz, dt, nt, fc, pad, component=2, invert="vs", scale=1.0, sos=None,
+                     n_taper=0, fd_order=2, free_surface=False, src_type="force", block_size=None,
+                     grad_smooth_sigma=None, source_taper=None, illumination=None, src_types=None):
+    """(g_Vs, g_Vp, g_rho) on the physical grid and the loss
+    scale * mean_shots mean_{t,r}(F T (pred - obs))^2 (FP64)."""
+    if backend not in _BACKENDS:
+        raise ValueError(f"unknown backend {backend!r}; use 'cuda' or 'cuda_imaging'")
+    if invert not in ("vs", "vs_vp", "all"):
+        raise ValueError(f"invert={invert!r}; use 'vs', 'vs_vp', or 'all'")
+    if invert == "all":
+        raise NotImplementedError("invert='all': the density gradient is not accumulated on the GPU")
+    if fd_order not in (2, 4, 8):
+        raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
+    mode = _BACKENDS[backend]
+    sx = np.atleast_1d(np.asarray(src_x)).astype(np.int64)
+    sz = np.broadcast_to(np.atleast_1d(np.asarray(src_z)), sx.shape).astype(np.int64)
+    types = list(src_types) if src_types is not None else [src_type] * sx.size
+    for t in types:
+        if t not in ("force", "moment"):
+            raise NotImplementedError(f"src_type={t!r} not supported (use 'force' or 'moment').")
+    rx = np.asarray(rec_x, dtype=np.int32).reshape(-1)
+    rz = np.asarray(rec_z, dtype=np.int32).reshape(-1)
+    S = _solver(int(nz_dom), int(nx_dom), dx, dz, dt, int(nt), fc, int(pad), rx.size, sx.size, int(fd_order),
+                free_surface)
+    S.set_receivers(rx, rz)
+    S.set_shots(sx, sz, types, np.asarray(src_wavelet, dtype=np.float32))
+    S.set_model(Vs, Vp, rho)
+    S.forward(store=True)
+    loss = float(S.misfit(observed, component, scale, sos, n_taper).sum())
+    g = S.gradient(exact=(mode == "exact"), imaging=(mode == "imaging"))[mode]
+    g_vs, g_vp, g_rho = (np.array(a) for a in g)
+    if invert == "vs":
+        g_vp = np.zeros_like(g_vp)
+    g_rho = np.zeros_like(g_rho)
+    return _postprocess((g_vs, g_vp, g_rho), grad_smooth_sigma, source_taper, illumination), loss

@@ -1,0 +1,42 @@
+"""Host-side pieces of the reference-signature API (CPU)."""
+import numpy as np
+
+from oracle import oracle as O
+
+
+def test_filters_and_smoothing_match_the_oracle():
+    from scipy.signal import butter
+    from stfwi_b200 import fwi
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((400, 7))
+    sos = butter(6, 3.0, fs=1 / 0.002, output="sos")
+    np.testing.assert_allclose(fwi.sosfilt(x, sos), O.sosfilt(x, sos), rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(fwi.cosine_taper_end(x, 40), O.cosine_taper_end(x, 40), rtol=1e-12)
+    assert np.array_equal(fwi.cosine_taper_end(x, 0), x)
+    f = rng.standard_normal((30, 41))
+    np.testing.assert_allclose(fwi.gaussian_smooth_2d(f, 1.5), O.gaussian_smooth_2d(f, 1.5), rtol=1e-12)
+
+
+def test_ricker_matches_the_reference_formula():
+    from stfwi_b200 import fwi
+    from stfwi_b200 import models as Mo
+    t = np.arange(500) * 0.002
+    w = fwi.ricker_jax(t, 6.0, 0.25)
+    np.testing.assert_allclose(w, O.ricker(t, 6.0, 0.25), rtol=1e-14)
+    np.testing.assert_allclose(w, Mo.ricker(t, 6.0, 0.25), rtol=1e-14)
+    assert abs(w.max() - 1.0) < 1e-3
+
+
+def test_layered_fault_model_ranges():
+    from stfwi_b200 import models as Mo
+    vs, vp, rho = Mo.layered_fault_model(152, 500, seed=3)
+    assert vs.shape == (152, 500) and vs.dtype == np.float32
+    assert 1500 <= vp.min() and vp.max() <= 4700
+    assert 800 <= vs.min() and vs.max() <= 2750
+    assert 1700 <= rho.min() and rho.max() <= 2600
+    assert np.all(vp / vs >= 1.2 - 1e-6)
+    vs0, vp0, rho0 = Mo.smooth_initial(vs, vp, rho, 10.0)
+    assert np.abs(np.diff(vs0, axis=0)).max() < np.abs(np.diff(vs, axis=0)).max()
+    # config 1 / 2 are stable: CFL number below 1
+    for cfg in (Mo.CONFIG1, Mo.CONFIG2):
+        assert Mo.cfl_number(4700, cfg["dt"], cfg["dx"], cfg["dz"], cfg["fd_order"]) < 0.7
