@@ -63,7 +63,9 @@ typedef struct {
     int32_t shot_group;     /* shots per block (0: automatic) */
     double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
     int32_t kernel_variant; /* 0: TMA-pipelined tiles (default), 1: plain shared-memory tiles */
-    int32_t reserved0;
+    int32_t ckpt_interval;  /* gradient history: 0 = keep every step if it fits the budget, else
+                               checkpoint the state every k steps and recompute each k-step
+                               segment during the adjoint (k chosen to fit); k > 0 = that k */
 } stfwi_desc;
 
 /* source types */
@@ -91,6 +93,8 @@ typedef struct {
     const double *sos; /* host pointer, [nsos][6] */
 } stfwi_misfit_desc;
 
+/* Device bytes stfwi_create allocates for d (with ckpt_interval = 0: the
+ * every-step history). */
 size_t stfwi_workspace_bytes(const stfwi_desc *d);
 stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out);
 void stfwi_destroy(stfwi_handle *h);

@@ -38,7 +38,7 @@ class StfwiDesc(ct.Structure):
         ("nrec", ct.c_int32), ("max_shots", ct.c_int32),
         ("dx", ct.c_double), ("dz", ct.c_double), ("dt", ct.c_double), ("fc", ct.c_double),
         ("want_gradient", ct.c_int32), ("shot_group", ct.c_int32), ("mem_budget_gb", ct.c_double),
-        ("kernel_variant", ct.c_int32), ("reserved0", ct.c_int32),
+        ("kernel_variant", ct.c_int32), ("ckpt_interval", ct.c_int32),
     ]
 
 

@@ -231,8 +231,9 @@ __global__ void __launch_bounds__(NTHR) k_fwd_vel(Geo g, Mat m, Shots sh, float 
 struct FwdOut {
     float *rec;          // [nshot][4][nt][nrec]
     float *snap;         // strain history: + (s*slots + slot)*3*nd, or null
-    float *row0;         // post-PML d(vx)/dx at row 0 (free surface): + (s*slots+slot)*nx_dom, or null
-    int slots, slot;
+    float *row0;         // post-PML d(vx)/dx at row 0 (free surface): + (s*slots+slot_row0)*nx_dom, or null
+    int slots, slot;     // history slot written by this step (its carry-out)
+    int slot_row0;       // row-0 slot of this step
     double *energy;      // illumination accumulator [nz][nx] (padded grid, pitch nx), or null
     int energy_comp;     // 0 vx, 1 vz, 2 exx, 3 ezz
     int *status;         // bit 0: non-finite receiver sample
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(NTHR) k_fwd_str(Geo g, Mat m, Shots sh, Recv r
                 __stcs(sp + 2 * g.nd, esn);
             }
             if (out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
-                out.row0[((long long)s * out.slots + out.slot) * g.nx_dom + pj] = dxu;
+                out.row0[((long long)s * out.slots + out.slot_row0) * g.nx_dom + pj] = dxu;
             if (out.energy) {
                 float f = out.energy_comp == 2 ? exn : out.energy_comp == 3 ? ezn
                         : out.energy_comp == 0 ? U[o] : V[o];

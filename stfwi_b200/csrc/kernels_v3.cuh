@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V3_MINBLOCKS_HEAVY)
                 __stcs(sp + 2 * g.nd, axz);
             }
             if (out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
-                out.row0[((long long)s * out.slots + out.slot) * g.nx_dom + pj] = dxu;
+                out.row0[((long long)s * out.slots + out.slot_row0) * g.nx_dom + pj] = dxu;
             if (out.energy) {
                 float f;
                 if (out.energy_comp < 2) {

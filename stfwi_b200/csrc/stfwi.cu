@@ -75,6 +75,11 @@ struct stfwi_handle {
     float *rec = nullptr, *rec_adj = nullptr;
     float *snap = nullptr, *row0 = nullptr;
     int slots = 0;
+    // checkpointing: history of ck steps (slots = ck + 1, slot 0 = carry-in of
+    // the segment); ncp > 0 state checkpoints every ck steps (ncp = 0: the
+    // history covers all nt steps)
+    int ck = 0, ncp = 0;
+    float *CKF = nullptr, *CKPX = nullptr, *CKPZ = nullptr;
     double *acc = nullptr, *accLr = nullptr, *gtmp = nullptr;
     double *energy = nullptr;
     double *mis_trace = nullptr, *mis_shot = nullptr;
@@ -120,8 +125,8 @@ stfwi_status fail(stfwi_handle *h, stfwi_status st, const char *fmt, ...)
 struct Plan {
     long long nz, nx, P, nd, zs_n, xs_n;
     int tiles_x, tiles_z;
-    size_t fields, psi, snap, row0, acc, rec, misc;
-    size_t total() const { return fields + psi + snap + row0 + acc + rec + misc; }
+    size_t fields, psi, snap, row0, acc, rec, misc, ckpt;
+    size_t total() const { return fields + psi + snap + row0 + acc + rec + misc + ckpt; }
 };
 
 int auto_groups(const stfwi_desc *d, int tiles)
@@ -133,7 +138,8 @@ int auto_groups(const stfwi_desc *d, int tiles)
     return std::min(want, std::max(1, d->max_shots));
 }
 
-Plan make_plan(const stfwi_desc *d)
+// k: history segment length (k = nt: every step kept, no checkpoints)
+Plan make_plan(const stfwi_desc *d, int k)
 {
     Plan p{};
     p.nx = d->nx_dom + 2LL * d->pad;
@@ -148,8 +154,10 @@ Plan make_plan(const stfwi_desc *d)
     const int G = auto_groups(d, p.tiles_x * p.tiles_z);
     p.fields = (size_t)2 * S * F_N * p.nz * p.P * sizeof(float);
     p.psi = (size_t)S * (NPX * p.nz * p.xs_n + NPZ * p.zs_n * p.P) * sizeof(float);
-    p.snap = d->want_gradient ? (size_t)S * d->nt * 3 * p.nd * sizeof(float) : 0;
-    p.row0 = (d->want_gradient && d->free_surface) ? (size_t)S * d->nt * d->nx_dom * sizeof(float) : 0;
+    p.snap = d->want_gradient ? (size_t)S * (k + 1) * 3 * p.nd * sizeof(float) : 0;
+    p.row0 = (d->want_gradient && d->free_surface) ? (size_t)S * (k + 1) * d->nx_dom * sizeof(float) : 0;
+    const long long ncp = (d->want_gradient && k < d->nt) ? (d->nt + k - 1) / k : 0;
+    p.ckpt = (size_t)ncp * S * (F_N * p.nz * p.P + PX_NFWD * p.nz * p.xs_n + PZ_NFWD * p.zs_n * p.P) * sizeof(float);
     p.acc = (size_t)G * (5 * p.nd + d->nx_dom) * sizeof(double) + 3 * p.nd * 2 * sizeof(double);
     p.rec = (size_t)2 * S * 4 * d->nt * std::max(d->nrec, 1) * sizeof(float)
           + (size_t)S * d->nt * std::max(d->nrec, 1) * sizeof(float);
@@ -497,6 +505,58 @@ stfwi_status zero_adjoint_state(stfwi_handle *h, cudaStream_t st)
     return STFWI_OK;
 }
 
+// history slot 0 of every shot = the physical cells of the current state
+// (the carry-in of the first step of a history segment)
+__global__ void k_snap_state(Geo g, int slots, const float *F, float *snap)
+{
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (q >= g.nd) return;
+    const int pi = (int)(q / g.nx_dom), pj = (int)(q % g.nx_dom);
+    const long long o = (long long)(pi + g.z0) * g.P + pj + g.pad;
+    float *dst = snap + (long long)s * slots * 3 * g.nd + q;
+#pragma unroll
+    for (int f = 0; f < 3; ++f) dst[f * g.nd] = F[((long long)s * F_N + F_EX + f) * g.fstride + o];
+}
+
+void snap_state(stfwi_handle *h, cudaStream_t st)
+{
+    const Geo &g = h->g;
+    k_snap_state<<<dim3((unsigned)((g.nd + 255) / 256), h->nshot), 256, 0, st>>>(g, h->slots, h->F, h->snap);
+}
+
+// state of the forward (fields + forward C-PML memories) <-> checkpoint c
+stfwi_status copy_ckpt(stfwi_handle *h, int c, bool save, cudaStream_t st)
+{
+    const Geo &g = h->g;
+    const size_t S = (size_t)h->d.max_shots, ns = (size_t)h->nshot;
+    float *cf = h->CKF + (size_t)c * S * F_N * g.fstride;
+    float *cx = h->CKPX + (size_t)c * S * PX_NFWD * g.xstride;
+    float *cz = h->CKPZ + (size_t)c * S * PZ_NFWD * g.zstride;
+    const size_t fb = ns * F_N * g.fstride * 4;
+    const size_t xw = PX_NFWD * g.xstride * 4, xp = NPX * g.xstride * 4;
+    const size_t zw = PZ_NFWD * g.zstride * 4, zp = NPZ * g.zstride * 4;
+    if (save) {
+        CK(h, cudaMemcpyAsync(cf, h->F, fb, cudaMemcpyDeviceToDevice, st));
+        CK(h, cudaMemcpy2DAsync(cx, xw, h->PX, xp, xw, ns, cudaMemcpyDeviceToDevice, st));
+        CK(h, cudaMemcpy2DAsync(cz, zw, h->PZ, zp, zw, ns, cudaMemcpyDeviceToDevice, st));
+    } else {
+        CK(h, cudaMemcpyAsync(h->F, cf, fb, cudaMemcpyDeviceToDevice, st));
+        CK(h, cudaMemcpy2DAsync(h->PX, xp, cx, xw, xw, ns, cudaMemcpyDeviceToDevice, st));
+        CK(h, cudaMemcpy2DAsync(h->PZ, zp, cz, zw, zw, ns, cudaMemcpyDeviceToDevice, st));
+    }
+    return STFWI_OK;
+}
+
+void fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+{
+    switch (h->d.fd_order) {
+    case 2: launch_fwd_step<2>(h, n, o, st); break;
+    case 4: launch_fwd_step<4>(h, n, o, st); break;
+    default: launch_fwd_step<8>(h, n, o, st); break;
+    }
+}
+
 // record the whole forward pass (kind 0) or illumination pass (kind 2)
 stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStream_t st)
 {
@@ -512,15 +572,19 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
         o.energy = h->energy;
         o.energy_comp = comp;
     }
+    // with checkpoints the history is written later, segment by segment
+    const bool hist = store && h->ncp == 0;
+    if (hist) snap_state(h, st);
     for (int n = 0; n < h->g.nt; ++n) {
-        o.snap = store ? h->snap : nullptr;
-        o.row0 = (store && h->g.fs) ? h->row0 : nullptr;
-        o.slot = n;
-        switch (h->d.fd_order) {
-        case 2: launch_fwd_step<2>(h, n, o, st); break;
-        case 4: launch_fwd_step<4>(h, n, o, st); break;
-        default: launch_fwd_step<8>(h, n, o, st); break;
+        if (store && h->ncp > 0 && n % h->ck == 0) {
+            stfwi_status r = copy_ckpt(h, n / h->ck, true, st);
+            if (r) return r;
         }
+        o.snap = hist ? h->snap : nullptr;
+        o.row0 = (hist && h->g.fs) ? h->row0 : nullptr;
+        o.slot = n + 1;
+        o.slot_row0 = n;
+        fwd_step(h, n, o, st);
     }
     CK(h, cudaGetLastError());
     return STFWI_OK;
@@ -655,8 +719,9 @@ void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t)
 
 size_t stfwi_workspace_bytes(const stfwi_desc *d)
 {
-    if (!d) return 0;
-    return make_plan(d).total();
+    if (!d || d->nt < 1) return 0;
+    const int k = d->ckpt_interval > 0 ? std::min(d->ckpt_interval, d->nt) : d->nt;
+    return make_plan(d, k).total();
 }
 
 const char *stfwi_last_error(const stfwi_handle *h) { return h ? h->err.c_str() : "null handle"; }
@@ -672,7 +737,6 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_INVALID;
     stfwi_handle *h = new stfwi_handle();
     h->d = *d;
-    Plan p = make_plan(d);
     cudaGetDevice(&h->device);
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
@@ -680,6 +744,22 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_CUDA;
     }
     const double budget = d->mem_budget_gb > 0 ? d->mem_budget_gb * 1e9 : 0.85 * (double)fr;
+    // history plan: every step if it fits, else the longest checkpoint
+    // segment that fits (the recompute costs one forward whatever k is)
+    int k = d->nt;
+    if (d->want_gradient) {
+        if (d->ckpt_interval > 0) {
+            k = std::min(d->ckpt_interval, d->nt);
+        } else if ((double)make_plan(d, d->nt).total() > budget) {
+            k = 0;
+            for (int kk = d->nt - 1; kk >= 1; --kk)
+                if ((double)make_plan(d, kk).total() <= budget) { k = kk; break; }
+            if (k == 0) k = 1;
+        }
+    }
+    Plan p = make_plan(d, k);
+    h->ck = k;
+    h->ncp = (d->want_gradient && k < d->nt) ? (d->nt + k - 1) / k : 0;
     if ((double)p.total() > budget) {
         h->err = "workspace of " + std::to_string(p.total() / 1e9) + " GB exceeds the budget of " +
                  std::to_string(budget / 1e9) + " GB";
@@ -720,7 +800,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         h->acc_groups = h->groups;
     }
     h->acc_used = h->acc_groups;
-    h->slots = d->nt;
+    h->slots = k + 1;
 
     auto alloc = [&](void **ptr, size_t bytes) -> bool {
         if (bytes == 0) { *ptr = nullptr; return true; }
@@ -751,6 +831,11 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
           alloc((void **)&h->rec_adj, (size_t)S * 4 * d->nt * nrec * 4) &&
           alloc((void **)&h->obs, (size_t)S * d->nt * nrec * 4);
     ok &= alloc((void **)&h->snap, p.snap) && alloc((void **)&h->row0, p.row0);
+    if (h->ncp > 0) {
+        ok &= alloc((void **)&h->CKF, (size_t)h->ncp * S * F_N * NP * 4) &&
+              alloc((void **)&h->CKPX, (size_t)h->ncp * S * PX_NFWD * p.nz * p.xs_n * 4) &&
+              alloc((void **)&h->CKPZ, (size_t)h->ncp * S * PZ_NFWD * p.zs_n * p.P * 4);
+    }
     ok &= alloc((void **)&h->acc, (size_t)h->acc_groups * 5 * nd * 8) &&
           alloc((void **)&h->accLr, (size_t)std::max(h->acc_groups, d->max_shots) * std::max(d->nx_dom, 1) * 8) &&
           alloc((void **)&h->gtmp, (size_t)6 * nd * 8);
@@ -794,7 +879,8 @@ void stfwi_destroy(stfwi_handle *h)
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
                     h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
-                    h->mis_trace, h->mis_shot, h->src_a, h->tile_start64, h->tile_rec64};
+                    h->mis_trace, h->mis_shot, h->src_a, h->tile_start64, h->tile_rec64, h->CKF, h->CKPX,
+                    h->CKPZ};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (int k = 0; k < 4; ++k)
@@ -1025,13 +1111,13 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
         const int thr = 256;
         if (g.nrec > 0)
             k_inject_last<<<(g.nshot * g.nrec + thr - 1) / thr, thr, 0, s>>>(g, h->rx, h->rz, h->rec_adj, h->A);
-        for (int n = g.nt - 1; n >= 0; --n) {
+        auto adj = [&](int n, int seg0) {
             const int ping = (g.nt - 1 - n) & 1;
             AdjIn ai{};
-            ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = n;
+            ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = n - seg0;
             ai.accLr = h->accLr; ai.want_exact = ex; ai.ping = ping;
             AdjOut ao{};
-            ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = n - 1; ao.slot_img = n;
+            ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = n - seg0; ao.slot_img = n - seg0 + 1;
             ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im;
             ao.src_a = sr ? src_dev : nullptr; ao.rec_adj = h->rec_adj; ao.ping = ping;
             switch (h->d.fd_order) {
@@ -1039,6 +1125,27 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
             case 4: launch_adj_step<4>(h, n, ai, ao, s); break;
             default: launch_adj_step<8>(h, n, ai, ao, s); break;
             }
+        };
+        if ((ex || im) && h->ncp > 0) {
+            // segments from the last: restore the checkpoint, recompute the
+            // segment's history, run its adjoint steps
+            for (int c = h->ncp - 1; c >= 0; --c) {
+                const int seg0 = c * h->ck, seg1 = std::min(seg0 + h->ck, g.nt);
+                r = copy_ckpt(h, c, false, s);
+                if (r) return r;
+                snap_state(h, s);
+                FwdOut o{};
+                o.rec = h->rec; o.status = h->status; o.slots = h->slots;
+                o.snap = h->snap; o.row0 = g.fs ? h->row0 : nullptr;
+                for (int n = seg0; n < seg1; ++n) {
+                    o.slot = n - seg0 + 1;
+                    o.slot_row0 = n - seg0;
+                    fwd_step(h, n, o, s);
+                }
+                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0);
+            }
+        } else {
+            for (int n = g.nt - 1; n >= 0; --n) adj(n, 0);
         }
         if (ex || im)
             k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->acc_used, h->lr_used, h->acc, h->accLr, h->L2M,

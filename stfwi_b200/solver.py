@@ -46,14 +46,15 @@ class Solver:
 
     def __init__(self, nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, max_shots, fd_order=2,
                  free_surface=True, want_gradient=True, shot_group=0, mem_budget_gb=0.0,
-                 kernel_variant=0):
+                 kernel_variant=0, ckpt_interval=0):
         if fd_order not in (2, 4, 8):
             raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
         self.lib = N.load()
         self.desc = N.StfwiDesc(int(nz_dom), int(nx_dom), int(pad), int(fd_order),
                                 int(bool(free_surface)), int(nt), int(nrec), int(max_shots),
                                 float(dx), float(dz), float(dt), float(fc), int(bool(want_gradient)),
-                                int(shot_group), float(mem_budget_gb), int(kernel_variant), 0)
+                                int(shot_group), float(mem_budget_gb), int(kernel_variant),
+                                int(ckpt_interval))
         h = ct.c_void_p()
         st = self.lib.stfwi_create(ct.byref(self.desc), ct.byref(h))
         if st != N.STFWI_OK:
@@ -78,7 +79,7 @@ class Solver:
                         int(kw.get("free_surface", True)), kw["nt"], kw["nrec"], kw["max_shots"],
                         kw["dx"], kw["dz"], kw["dt"], kw["fc"], int(kw.get("want_gradient", True)),
                         kw.get("shot_group", 0), kw.get("mem_budget_gb", 0.0),
-                        kw.get("kernel_variant", 0), 0)
+                        kw.get("kernel_variant", 0), kw.get("ckpt_interval", 0))
         return int(lib.stfwi_workspace_bytes(ct.byref(d)))
 
     # ------------------------------------------------------------------ helpers

@@ -35,6 +35,10 @@ def test_workspace_and_grid_shape_are_host_only():
     ws = lib.stfwi_workspace_bytes(ct.byref(d))
     # the strain history dominates: 50 shots x 2000 steps x 3 x 76000 cells x 4 B
     assert 91e9 < ws < 95e9
+    d.ckpt_interval = 200  # checkpoints every 200 steps: 10 x state + a 201-step history
+    ws_ck = lib.stfwi_workspace_bytes(ct.byref(d))
+    assert 9e9 < ws_ck < 14e9, ws_ck
+    d.ckpt_interval = 0
     d.want_gradient = 0
     assert lib.stfwi_workspace_bytes(ct.byref(d)) < 2e9
 
