@@ -58,9 +58,12 @@ def _postprocess(grads, grad_smooth_sigma, source_taper, illumination):
 def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observed, rec_x, rec_z, nx_dom,
                      nz_dom, dx, dz, dt, nt, fc, pad, component=2, invert="vs", scale=1.0, sos=None,
                      n_taper=0, fd_order=2, free_surface=False, src_type="force", block_size=None,
-                     grad_smooth_sigma=None, source_taper=None, illumination=None, src_types=None):
+                     grad_smooth_sigma=None, source_taper=None, illumination=None, src_types=None,
+                     n_shots_total=None):
     """(g_Vs, g_Vp, g_rho) on the physical grid and the loss
-    scale * mean_shots mean_{t,r}(F T (pred - obs))^2 (FP64)."""
+    scale * mean_shots mean_{t,r}(F T (pred - obs))^2 (FP64).  With
+    ``n_shots_total`` the mean over shots divides by that count (these shots
+    are one shard of a larger batch)."""
     if backend not in _BACKENDS:
         raise ValueError(f"unknown backend {backend!r}; use 'cuda' or 'cuda_imaging'")
     if invert not in ("vs", "vs_vp", "all"):
@@ -84,7 +87,7 @@ def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observe
     S.set_shots(sx, sz, types, np.asarray(src_wavelet, dtype=np.float32))
     S.set_model(Vs, Vp, rho)
     S.forward(store=True)
-    loss = float(S.misfit(observed, component, scale, sos, n_taper).sum())
+    loss = float(S.misfit(observed, component, scale, sos, n_taper, nshot_norm=n_shots_total or 0).sum())
     g = S.gradient(exact=(mode == "exact"), imaging=(mode == "imaging"))[mode]
     g_vs, g_vp, g_rho = (np.array(a) for a in g)
     if invert == "vs":
