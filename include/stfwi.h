@@ -62,7 +62,8 @@ typedef struct {
     int32_t want_gradient;  /* 1: reserve strain history + accumulators */
     int32_t shot_group;     /* shots per block (0: automatic) */
     double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
-    int32_t kernel_variant; /* 0: TMA-pipelined tiles (default), 1: plain shared-memory tiles */
+    int32_t kernel_variant; /* 0: two-column TMA-pipelined tiles (default), 1: plain shared-memory tiles,
+                               2: one-column TMA-pipelined tiles */
     int32_t ckpt_interval;  /* gradient history: 0 = keep every step if it fits the budget, else
                                checkpoint the state every k steps and recompute each k-step
                                segment during the adjoint (k chosen to fit); k > 0 = that k */

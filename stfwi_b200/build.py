@@ -7,7 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libstfwi.so")
 SOURCES = [os.path.join(HERE, "csrc", "stfwi.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", "kernels.cuh"), os.path.join(ROOT, "include", "stfwi.h")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "kernels_v3.cuh", "kernels_v4.cuh", "tma.cuh")] \
+    + [os.path.join(ROOT, "include", "stfwi.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

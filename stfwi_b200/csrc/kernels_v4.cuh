@@ -1,0 +1,992 @@
+// Two-column register-blocked stencil kernels (sm_100a), the default path.
+//
+// The same four phases, state variables and arithmetic as kernels_v3.cuh
+// (stress-state forward, buoyancy-scaled adjoint; kernels.cuh documents the
+// correspondence with the reference), with each thread owning TWO adjacent
+// columns of RPT rows: a tile is 64 columns wide, the x-neighbourhood of a
+// thread's two columns on one row is five aligned float2 shared loads
+// (columns j-4 .. j+5), and the z-stencils come from a float2 register
+// window of RPT + 2K rows.  Halo tiles arrive by TMA (one 4-D bulk tensor
+// copy per shot, double-buffered over the shots a block owns).
+#pragma once
+#include "kernels_v3.cuh"
+
+namespace stfwi {
+
+#ifndef STFWI_V4_MINBLOCKS
+#define STFWI_V4_MINBLOCKS 2
+#endif
+
+constexpr int TX4 = 64;               // tile width: 32 lanes x 2 columns
+constexpr int XO4 = 4;                // x halo of the staged tile
+constexpr int SW4 = TX4 + 2 * XO4;    // 72 floats = 288 B rows
+
+template <int FD, int RPT> struct G4 {
+    static constexpr int K = FD / 2;
+    static constexpr int TZH = RPT * NWARP;
+    static constexpr int SH = TZH + 2 * K;
+    static constexpr int SN = SH * SW4;
+    static constexpr int W = RPT + 2 * K;
+    static constexpr int M = 2 * K + 1;
+    static constexpr int S1 = al32_3(SN), S2 = al32_3(2 * SN), S3 = al32_3(3 * SN);
+};
+
+constexpr int RPT4 = 4;    // rows per thread: fwd_vel, fwd_str, adj_a
+constexpr int RPT4B = 2;   // rows per thread: adj_b (FP64 sums per cell in registers)
+
+template <int FD> struct L4 {
+    using A = G4<FD, RPT4>;
+    using B = G4<FD, RPT4B>;
+    static constexpr int VEL = 2 * A::S3;
+    static constexpr int STR = 2 * A::S2;
+    static constexpr int ADA = 2 * A::S3 + A::S1;
+    static constexpr int ADB = 2 * B::S2 + 2 * B::S1;
+    static constexpr size_t bytes(int floats, int nbar) { return (size_t)floats * 4 + 8 * nbar; }
+};
+
+// a[i] = f[j - 4 + i], i in [0, 10): the x-neighbourhood of columns j, j+1
+__device__ __forceinline__ void xrow(float (&a)[10], const float *s, int q)
+{
+    const float2 *p = reinterpret_cast<const float2 *>(s + q - 4);
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const float2 t = p[m];
+        a[2 * m] = t.x;
+        a[2 * m + 1] = t.y;
+    }
+}
+
+// stencils on a (output column c of the pair, global column jc)
+template <int FD, bool MASK>
+__device__ __forceinline__ float a_dp(const float (&a)[10], int c, int jc, int n)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= FD / 2; ++k)
+        if (!MASK || mP(jc, k, n)) d += cf<FD>(k) * (a[4 + c + k] - a[5 + c - k]);
+    return d;
+}
+template <int FD, bool MASK>
+__device__ __forceinline__ float a_dm(const float (&a)[10], int c, int jc, int n)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= FD / 2; ++k)
+        if (!MASK || mM(jc, k, n)) d += cf<FD>(k) * (a[3 + c + k] - a[4 + c - k]);
+    return d;
+}
+template <int FD, bool MASK>
+__device__ __forceinline__ float a_tdp(const float (&a)[10], int c, int jc, int n)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= FD / 2; ++k) {
+        if (!MASK || mP(jc - k, k, n)) d += cf<FD>(k) * a[4 + c - k];
+        if (!MASK || mP(jc + k - 1, k, n)) d -= cf<FD>(k) * a[3 + c + k];
+    }
+    return d;
+}
+template <int FD, bool MASK>
+__device__ __forceinline__ float a_tdm(const float (&a)[10], int c, int jc, int n, int lim)
+{
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= FD / 2; ++k) {
+        const int t1 = jc - k + 1, t2 = jc + k;
+        if (!MASK || (mM(t1, k, n) && t1 < lim)) d += cf<FD>(k) * a[5 + c - k];
+        if (!MASK || (mM(t2, k, n) && t2 < lim)) d -= cf<FD>(k) * a[4 + c + k];
+    }
+    return d;
+}
+
+// z window of the pair: w[m][c] = f(row ty*RPT + m - K relative to the tile, column c)
+template <int W, int RPT>
+__device__ __forceinline__ void zwin2(float (&w)[W][2], const float *s, int ty, int tx)
+{
+#pragma unroll
+    for (int m = 0; m < W; ++m) {
+        const float2 t = *reinterpret_cast<const float2 *>(s + (ty * RPT + m) * SW4 + XO4 + 2 * tx);
+        w[m][0] = t.x;
+        w[m][1] = t.y;
+    }
+}
+template <int FD, bool MASK, int W>
+__device__ __forceinline__ float w_dp(const float (&w)[W][2], int r, int c, int i, int n)
+{
+    constexpr int K = FD / 2;
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= K; ++k)
+        if (!MASK || mP(i, k, n)) d += cf<FD>(k) * (w[r + K + k][c] - w[r + K - k + 1][c]);
+    return d;
+}
+template <int FD, bool MASK, int W>
+__device__ __forceinline__ float w_dm(const float (&w)[W][2], int r, int c, int i, int n)
+{
+    constexpr int K = FD / 2;
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= K; ++k)
+        if (!MASK || mM(i, k, n)) d += cf<FD>(k) * (w[r + K + k - 1][c] - w[r + K - k][c]);
+    return d;
+}
+template <int FD, bool MASK, int W>
+__device__ __forceinline__ float w_tdp(const float (&w)[W][2], int r, int c, int i, int n)
+{
+    constexpr int K = FD / 2;
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        if (!MASK || mP(i - k, k, n)) d += cf<FD>(k) * w[r + K - k][c];
+        if (!MASK || mP(i + k - 1, k, n)) d -= cf<FD>(k) * w[r + K + k - 1][c];
+    }
+    return d;
+}
+template <int FD, bool MASK, int W>
+__device__ __forceinline__ float w_tdm(const float (&w)[W][2], int r, int c, int i, int n, int lim)
+{
+    constexpr int K = FD / 2;
+    float d = 0.f;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) {
+        const int t1 = i - k + 1, t2 = i + k;
+        if (!MASK || (mM(t1, k, n) && t1 < lim)) d += cf<FD>(k) * w[r + K - k + 1][c];
+        if (!MASK || (mM(t2, k, n) && t2 < lim)) d -= cf<FD>(k) * w[r + K + k][c];
+    }
+    return d;
+}
+
+__device__ __forceinline__ Ctx3 ctx4(const Geo &g, int spg, int tzh, int tiles_x)
+{
+    Ctx3 c;
+    c.tile = blockIdx.x;
+    c.j0 = (c.tile % tiles_x) * TX4;
+    c.i0 = (c.tile / tiles_x) * tzh;
+    c.s0 = blockIdx.y * spg;
+    c.s1 = min(c.s0 + spg, g.nshot);
+    return c;
+}
+
+__device__ __forceinline__ bool box_special4(const Geo &g, int i0, int j0, int tzh, int K)
+{
+    const int r0 = i0 - K, r1 = i0 + tzh + K - 1, c0 = j0 - XO4, c1 = j0 + TX4 + XO4 - 1;
+    if (c0 < g.pad || c1 >= g.nx - g.pad) return true;
+    if (r1 >= g.nz - g.pad) return true;
+    if (r0 <= 0) return true;
+    if (!g.fs && r0 < g.pad) return true;
+    return false;
+}
+
+// ------------------------------------------------------------- forward: velocities
+
+template <int FD>
+__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+    k4_fwd_vel(Geo g, Mat m, Shots sh, float *F, float *PX, float *PZ, int n, int spg, int tiles_x, int *status,
+               const __grid_constant__ CUtensorMap tmS)
+{
+    using T = G4<FD, RPT4>;
+    constexpr int K = T::K, SN = T::SN, RPT = RPT4;
+    extern __shared__ __align__(128) float sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::VEL);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const int nsh = c.s1 - c.s0;
+    if (nsh <= 0) return;
+    if (tid == 0) {
+        mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
+        fence_async_shared();
+        for (int b = 0; b < 2 && b < nsh; ++b) {
+            mbar_arrive_expect_tx(bar + b, 3 * SN * 4);
+            tma_load_4d(sm + b * T::S3, &tmS, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+        }
+    }
+    __syncthreads();
+    const int jb = c.j0 + 2 * tx;
+    int xs[2];
+    float bxv[2], axv[2], ikxv[2];
+    bool colin[2];
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+        const int j = jb + cc;
+        xs[cc] = (j < g.nx) ? xstrip_index(g, j) : -1;
+        bxv[cc] = xs[cc] >= 0 ? m.bx[j] : 0.f;
+        axv[cc] = xs[cc] >= 0 ? m.ax[j] : 0.f;
+        ikxv[cc] = xs[cc] >= 0 ? m.ikx[j] : 1.f;
+        colin[cc] = j >= T::M && j <= g.nx - 1 - T::M;
+    }
+    float Bc[RPT][2];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int i = c.i0 + ty * RPT + r, j = jb + cc;
+            Bc[r][cc] = (i < g.nz && j < g.nx) ? m.B[(long long)i * g.P + j] : 0.f;
+        }
+
+    for (int it = 0; it < nsh; ++it) {
+        const int s = c.s0 + it;
+        float *S = sm + (it & 1) * T::S3;
+        float *U = F + ((long long)s * F_N + F_U) * g.fstride;
+        float *V = F + ((long long)s * F_N + F_V) * g.fstride;
+        float u[RPT][2], v[RPT][2];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            const long long o = (long long)i * g.P + jb;
+            if (i < g.nz - 1 && jb < g.nx) {
+                const float2 a = *reinterpret_cast<const float2 *>(U + o);
+                const float2 b = *reinterpret_cast<const float2 *>(V + o);
+                u[r][0] = a.x; u[r][1] = a.y; v[r][0] = b.x; v[r][1] = b.y;
+            } else {
+                u[r][0] = u[r][1] = v[r][0] = v[r][1] = 0.f;
+            }
+        }
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
+            abort3(bar, 2, status);
+            return;
+        }
+        const float *sxx = S, *szz = S + SN, *sxz = S + 2 * SN;
+        float wxz[T::W][2], wzz[T::W][2];
+        zwin2<T::W, RPT>(wxz, sxz, ty, tx);
+        zwin2<T::W, RPT>(wzz, szz, ty, tx);
+        const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
+            float ax[10], az[10];
+            xrow(ax, sxx, q);
+            xrow(az, sxz, q);
+            const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
+            const int zs = zstrip_index(g, i);
+            float un[2], vn[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j = jb + cc;
+                un[cc] = u[r][cc];
+                vn[cc] = v[r][cc];
+                if (i >= g.nz - 1 || j < 1 || j >= g.nx - 1) continue;
+                float dxx, dzxz, dxxz, dzz;
+                if (colin[cc] && rowin) {
+                    dxx = a_dp<FD, false>(ax, cc, j, g.nx);
+                    dxxz = a_dm<FD, false>(az, cc, j, g.nx);
+                    dzxz = w_dm<FD, false>(wxz, r, cc, i, g.nz);
+                    dzz = w_dp<FD, false>(wzz, r, cc, i, g.nz);
+                } else {
+                    dxx = a_dp<FD, true>(ax, cc, j, g.nx);
+                    dxxz = a_dm<FD, true>(az, cc, j, g.nx);
+                    dzxz = w_dm<FD, true>(wxz, r, cc, i, g.nz);
+                    dzz = w_dp<FD, true>(wzz, r, cc, i, g.nz);
+                    if (g.fs && i == 0) dzxz = 2.f * cf<FD>(1) * wxz[r + K][cc];
+                }
+                if (xs[cc] >= 0) {
+                    dxx = pml_fwd(dxx, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_SXX) + (long long)i * g.xs_n + xs[cc]);
+                    dxxz = pml_fwd(dxxz, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_SXZ) + (long long)i * g.xs_n + xs[cc]);
+                }
+                if (zs >= 0) {
+                    const float b = m.bz[i], a = m.az[i], ik = m.ikz[i];
+                    dzxz = pml_fwd(dzxz, b, a, ik, pz_ptr(g, PZ, s, PZ_SXZ) + (long long)zs * g.P + j);
+                    dzz = pml_fwd(dzz, b, a, ik, pz_ptr(g, PZ, s, PZ_SZZ) + (long long)zs * g.P + j);
+                }
+                un[cc] = u[r][cc] + g.dtdx * Bc[r][cc] * dxx + g.dtdz * Bc[r][cc] * dzxz;
+                float vv = v[r][cc] + g.dtdx * Bc[r][cc] * dxxz + g.dtdz * Bc[r][cc] * dzz;
+                if (stype == 0 && i == ssz && j == ssx) vv = vv + sh.fcoef[s] * sh.wav[(long long)s * g.nt + n];
+                vn[cc] = vv;
+            }
+            // cells outside the update region keep their value (column 0, nx-1, row nz-1)
+            if (i < g.nz - 1 && jb < g.nx) {
+                const long long o = (long long)i * g.P + jb;
+                if (jb + 1 < g.nx) {
+                    *reinterpret_cast<float2 *>(U + o) = make_float2(un[0], un[1]);
+                    *reinterpret_cast<float2 *>(V + o) = make_float2(vn[0], vn[1]);
+                } else {
+                    U[o] = un[0];
+                    V[o] = vn[0];
+                }
+            }
+        }
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0 && it + 2 < nsh) {
+            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4);
+            tma_load_4d(S, &tmS, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_EX, s + 2);
+        }
+    }
+}
+
+// ------------------------------------------------------------- forward: stresses
+
+template <int FD, bool ENERGY>
+__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+    k4_fwd_str(Geo g, Mat m, Shots sh, Recv rv, float *F, float *PX, float *PZ, int n, int spg, int tiles_x,
+               FwdOut out, const __grid_constant__ CUtensorMap tmV)
+{
+    using T = G4<FD, RPT4>;
+    constexpr int K = T::K, SN = T::SN, RPT = RPT4;
+    extern __shared__ __align__(128) float sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::STR);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const int nsh = c.s1 - c.s0;
+    if (nsh <= 0) return;
+    if (tid == 0) {
+        mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
+        fence_async_shared();
+        for (int b = 0; b < 2 && b < nsh; ++b) {
+            mbar_arrive_expect_tx(bar + b, 2 * SN * 4);
+            tma_load_4d(sm + b * T::S2, &tmV, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+        }
+    }
+    __syncthreads();
+    const int jb = c.j0 + 2 * tx;
+    int xs[2];
+    float bxv[2], axv[2], ikxv[2], Lr0[2];
+    bool colin[2];
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+        const int j = jb + cc;
+        xs[cc] = (j < g.nx) ? xstrip_index(g, j) : -1;
+        bxv[cc] = xs[cc] >= 0 ? m.bx[j] : 0.f;
+        axv[cc] = xs[cc] >= 0 ? m.ax[j] : 0.f;
+        ikxv[cc] = xs[cc] >= 0 ? m.ikx[j] : 1.f;
+        Lr0[cc] = (g.fs && j < g.nx) ? m.Lr[j] : 0.f;
+        colin[cc] = j >= T::M && j <= g.nx - 1 - T::M;
+    }
+    float ml2m[RPT][2], ml[RPT][2], mm2[RPT][2];
+    constexpr int RG = ENERGY ? RPT : 1;
+    double eacc[RG][2];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int i = c.i0 + ty * RPT + r, j = jb + cc;
+            const long long o = (long long)i * g.P + j;
+            const bool ok = i < g.nz && j < g.nx;
+            ml2m[r][cc] = ok ? m.L2M[o] : 0.f;
+            ml[r][cc] = ok ? m.L[o] : 0.f;
+            mm2[r][cc] = ok ? 2.f * m.M[o] : 0.f;
+            if (r < RG) eacc[r][cc] = 0.0;
+        }
+
+    for (int it = 0; it < nsh; ++it) {
+        const int s = c.s0 + it;
+        float *S = sm + (it & 1) * T::S2;
+        float *sxx = F + ((long long)s * F_N + F_EX) * g.fstride;
+        float *szz = F + ((long long)s * F_N + F_EZ) * g.fstride;
+        float *sxz = F + ((long long)s * F_N + F_ES) * g.fstride;
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
+            abort3(bar, 2, out.status);
+            return;
+        }
+        const float *sU = S, *sV = S + SN;
+        float wU[T::W][2], wV[T::W][2];
+        zwin2<T::W, RPT>(wU, sU, ty, tx);
+        zwin2<T::W, RPT>(wV, sV, ty, tx);
+        const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            if (i >= g.nz) continue;
+            const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
+            float e1[2] = {0.f, 0.f}, e2[2] = {0.f, 0.f}, e3[2] = {0.f, 0.f};
+            if (jb < g.nx) {
+                const long long o = (long long)i * g.P + jb;
+                const float2 a = *reinterpret_cast<const float2 *>(sxx + o);
+                const float2 b = *reinterpret_cast<const float2 *>(szz + o);
+                const float2 d = *reinterpret_cast<const float2 *>(sxz + o);
+                e1[0] = a.x; e1[1] = a.y; e2[0] = b.x; e2[1] = b.y; e3[0] = d.x; e3[1] = d.y;
+            }
+            float au[10], av[10];
+            xrow(au, sU, q);
+            xrow(av, sV, q);
+            const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
+            const int zs = zstrip_index(g, i);
+            float nxx[2], nzz[2], nxz[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j = jb + cc;
+                nxx[cc] = e1[cc]; nzz[cc] = e2[cc]; nxz[cc] = e3[cc];
+                if (j >= g.nx) continue;
+                float dxu, dzv, dzu, dxv;
+                if (colin[cc] && rowin) {
+                    dxu = a_dm<FD, false>(au, cc, j, g.nx);
+                    dxv = a_dp<FD, false>(av, cc, j, g.nx);
+                    dzv = w_dm<FD, false>(wV, r, cc, i, g.nz);
+                    dzu = w_dp<FD, false>(wU, r, cc, i, g.nz);
+                } else {
+                    dxu = a_dm<FD, true>(au, cc, j, g.nx);
+                    dxv = a_dp<FD, true>(av, cc, j, g.nx);
+                    dzv = w_dm<FD, true>(wV, r, cc, i, g.nz);
+                    dzu = w_dp<FD, true>(wU, r, cc, i, g.nz);
+                }
+                if (j >= 1 && xs[cc] >= 0)
+                    dxu = pml_fwd(dxu, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_DXU) + (long long)i * g.xs_n + xs[cc]);
+                if (j < g.nx - 1) {
+                    if (g.fs && i == 0) dzv = Lr0[cc] * dxu * g.dzdx;
+                    if (zs >= 0)
+                        dzv = pml_fwd(dzv, m.bz[i], m.az[i], m.ikz[i], pz_ptr(g, PZ, s, PZ_DZV) + (long long)zs * g.P + j);
+                } else {
+                    dzv = 0.f;
+                }
+                if (j >= 1) {
+                    if (zs >= 0)
+                        dzu = pml_fwd(dzu, m.bz[i], m.az[i], m.ikz[i], pz_ptr(g, PZ, s, PZ_DZU) + (long long)zs * g.P + j);
+                } else {
+                    dzu = 0.f;
+                }
+                if (i < g.nz - 1) {
+                    if (xs[cc] >= 0)
+                        dxv = pml_fwd(dxv, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_DXV) + (long long)i * g.xs_n + xs[cc]);
+                } else {
+                    dxv = 0.f;
+                }
+                const float dex = (j >= 1) ? g.dtdx * dxu : 0.f;
+                const float dez = g.dtdz * dzv;
+                const float des = (i < g.nz - 1 && j < g.nx - 1) ? 0.5f * (g.dtdz * dzu + g.dtdx * dxv) : 0.f;
+                const float l2m = ml2m[r][cc], l = ml[r][cc];
+                float axx = e1[cc] + l2m * dex + l * dez;
+                float azz = e2[cc] + l * dex + l2m * dez;
+                const float axz = e3[cc] + mm2[r][cc] * des;
+                if (stype == 1 && i == ssz && j == ssx) {
+                    const float stm = sh.wav[(long long)s * g.nt + n] * g.dt / sh.mcoef[s];
+                    axx = axx + (l2m + l) * stm;
+                    azz = azz + (l + l2m) * stm;
+                }
+                nxx[cc] = axx; nzz[cc] = azz; nxz[cc] = axz;
+                const int pi = i - g.z0, pj = j - g.pad;
+                const bool phys = pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom;
+                if (out.snap && phys) {
+                    float *sp = out.snap + ((long long)s * out.slots + out.slot) * 3 * g.nd + (long long)pi * g.nx_dom + pj;
+                    __stcs(sp, axx);
+                    __stcs(sp + g.nd, azz);
+                    __stcs(sp + 2 * g.nd, axz);
+                }
+                if (out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
+                    out.row0[((long long)s * out.slots + out.slot_row0) * g.nx_dom + pj] = dxu;
+                if (ENERGY) {
+                    float f;
+                    if (out.energy_comp < 2) {
+                        f = out.energy_comp == 0 ? au[4 + cc] : av[4 + cc];
+                    } else {
+                        float ex, ez, es;
+                        strains_of(axx, azz, axz, l2m, l, 0.5f * mm2[r][cc], ex, ez, es);
+                        f = out.energy_comp == 2 ? ex : ez;
+                    }
+                    eacc[r % RG][cc] += (double)f * (double)f;
+                }
+            }
+            if (jb < g.nx) {
+                const long long o = (long long)i * g.P + jb;
+                if (jb + 1 < g.nx) {
+                    *reinterpret_cast<float2 *>(sxx + o) = make_float2(nxx[0], nxx[1]);
+                    *reinterpret_cast<float2 *>(szz + o) = make_float2(nzz[0], nzz[1]);
+                    *reinterpret_cast<float2 *>(sxz + o) = make_float2(nxz[0], nxz[1]);
+                } else {
+                    sxx[o] = nxx[0]; szz[o] = nzz[0]; sxz[o] = nxz[0];
+                }
+            }
+        }
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0 && it + 2 < nsh) {
+            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4);
+            tma_load_4d(S, &tmV, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
+        }
+        const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
+        const float *U = F + ((long long)s * F_N + F_U) * g.fstride;
+        const float *V = F + ((long long)s * F_N + F_V) * g.fstride;
+        for (int qq = r0 + tid; qq < r1; qq += NTHR) {
+            const int rid = rv.tile_rec[qq];
+            const long long o = (long long)rv.rz[rid] * g.P + rv.rx[rid];
+            float ex, ez, es;
+            strains_of(sxx[o], szz[o], sxz[o], m.L2M[o], m.L[o], m.M[o], ex, ez, es);
+            const float v0 = U[o], v1 = V[o];
+            float *dst = out.rec + (long long)s * 4 * g.nt * g.nrec + (long long)n * g.nrec + rid;
+            dst[0] = v0;
+            dst[(long long)g.nt * g.nrec] = v1;
+            dst[2LL * g.nt * g.nrec] = ex;
+            dst[3LL * g.nt * g.nrec] = ez;
+            if (!(isfinite(v0) && isfinite(v1) && isfinite(ex) && isfinite(ez))) atomicOr(out.status, 1);
+        }
+    }
+    if (ENERGY) {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int i = c.i0 + ty * RPT + r, j = jb + cc;
+                if (i < g.nz && j < g.nx) atomicAdd(out.energy + (long long)i * g.nx + j, eacc[r][cc]);
+            }
+    }
+}
+
+// ------------------------------------------------------------- adjoint: P = B U_a, Q = B V_a
+
+template <int FD>
+__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+    k4_adj_a(Geo g, Mat m, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x, AdjIn in,
+             int *status, const __grid_constant__ CUtensorMap tmE)
+{
+    using T = G4<FD, RPT4>;
+    constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4;
+    extern __shared__ __align__(128) float sm[];
+    float *aDxV = sm + 2 * T::S3;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADA);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const int nsh = c.s1 - c.s0;
+    if (nsh <= 0) return;
+    if (tid == 0) {
+        mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
+        fence_async_shared();
+        for (int b = 0; b < 2 && b < nsh; ++b) {
+            mbar_arrive_expect_tx(bar + b, 3 * SN * 4);
+            tma_load_4d(sm + b * T::S3, &tmE, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+        }
+    }
+    __syncthreads();
+    const bool fix = box_special4(g, c.i0, c.j0, T::TZH, K);
+    const int rd = in.ping, wr = 1 - in.ping;
+    const int jb = c.j0 + 2 * tx;
+    bool colin[2];
+    colin[0] = jb >= T::M && jb <= g.nx - 1 - T::M;
+    colin[1] = jb + 1 >= T::M && jb + 1 <= g.nx - 1 - T::M;
+    const float hdtdz = 0.5f * g.dtdz, hdtdx = 0.5f * g.dtdx;
+    float Bc[RPT][2];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int i = c.i0 + ty * RPT + r, j = jb + cc;
+            Bc[r][cc] = (i < g.nz && j < g.nx) ? m.B[(long long)i * g.P + j] : 0.f;
+        }
+    double glr[2] = {0.0, 0.0};
+
+    for (int it = 0; it < nsh; ++it) {
+        const int s = c.s0 + it;
+        float *S = sm + (it & 1) * T::S3;
+        float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
+        float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
+        float p[RPT][2], qv[RPT][2];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            const long long o = (long long)i * g.P + jb;
+            if (i < g.nz && jb < g.nx) {
+                const float2 a = *reinterpret_cast<const float2 *>(Pp + o);
+                const float2 b = *reinterpret_cast<const float2 *>(Qp + o);
+                p[r][0] = a.x; p[r][1] = a.y; qv[r][0] = b.x; qv[r][1] = b.y;
+            } else {
+                p[r][0] = p[r][1] = qv[r][0] = qv[r][1] = 0.f;
+            }
+        }
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
+            abort3(bar, 2, status);
+            return;
+        }
+        if (fix) {
+            const float *pDzU = pz_ptr(g, PZ, s, PZ_NFWD + rd * PZA_N + PZA_DZU);
+            const float *pDzV = pz_ptr(g, PZ, s, PZ_NFWD + rd * PZA_N + PZA_DZV);
+            const float *pDxU = px_ptr(g, PX, s, PX_NFWD + rd * PXA_N + PXA_DXU);
+            const float *pDxV = px_ptr(g, PX, s, PX_NFWD + rd * PXA_N + PXA_DXV);
+            float *wDzU = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_DZU);
+            float *wDzV = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_DZV);
+            float *wDxU = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_DXU);
+            float *wDxV = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_DXV);
+            for (int rr = ty; rr < SH; rr += NWARP) {
+                const int i = c.i0 - K + rr;
+                for (int cc = tx; cc < SW4; cc += TX) {
+                    const int jj = c.j0 - XO4 + cc, q = rr * SW4 + cc;
+                    const float ea = S[q], za = S[SN + q], sa = S[2 * SN + q];
+                    float vDxU = ea, vDzV = za, vDzU = sa, vDxV = sa;
+                    if (i >= 0 && i < g.nz && jj >= 0 && jj < g.nx) {
+                        const bool own = rr >= K && rr < K + T::TZH && cc >= XO4 && cc < XO4 + TX4;
+                        const int xs = xstrip_index(g, jj), zs = zstrip_index(g, i);
+                        if (zs >= 0) {
+                            const long long pz = (long long)zs * g.P + jj;
+                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i], ps = pDzV[pz];
+                            vDzV = (ik + a) * za + a * ps / g.dtdz;
+                            if (own) wDzV[pz] = b * (g.dtdz * za + ps);
+                        }
+                        float din = (jj >= 1) ? ea : 0.f;
+                        if (g.fs && i == 0 && jj < g.nx - 1) din = m.Lr[jj] * vDzV + din;
+                        vDxU = din;
+                        if (xs >= 0) {
+                            const long long px = (long long)i * g.xs_n + xs;
+                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj], ps = pDxU[px];
+                            vDxU = (ik + a) * din + a * ps / g.dtdx;
+                            if (own) wDxU[px] = b * (g.dtdx * din + ps);
+                        }
+                        const float h = (i < g.nz - 1 && jj < g.nx - 1) ? sa : 0.f;
+                        vDzU = h;
+                        vDxV = h;
+                        if (zs >= 0) {
+                            const long long pz = (long long)zs * g.P + jj;
+                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i], ps = pDzU[pz];
+                            vDzU = (ik + a) * h + a * ps / hdtdz;
+                            if (own) wDzU[pz] = b * (hdtdz * h + ps);
+                        }
+                        if (xs >= 0) {
+                            const long long px = (long long)i * g.xs_n + xs;
+                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj], ps = pDxV[px];
+                            vDxV = (ik + a) * h + a * ps / hdtdx;
+                            if (own) wDxV[px] = b * (hdtdx * h + ps);
+                        }
+                    }
+                    S[q] = vDxU; S[SN + q] = vDzV; S[2 * SN + q] = vDzU; aDxV[q] = vDxV;
+                }
+            }
+            __syncthreads();
+        }
+        const float *aDxU = S, *aDzV = S + SN, *aDzU = S + 2 * SN;
+        const float *aXV = fix ? aDxV : aDzU;
+        float wzu[T::W][2], wzv[T::W][2];
+        zwin2<T::W, RPT>(wzu, aDzU, ty, tx);
+        zwin2<T::W, RPT>(wzv, aDzV, ty, tx);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            if (i >= g.nz) continue;
+            const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
+            float ad[10], av[10];
+            xrow(ad, aDxU, q);
+            xrow(av, aXV, q);
+            const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
+            float np[2], nq[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j = jb + cc;
+                np[cc] = p[r][cc]; nq[cc] = qv[r][cc];
+                if (j >= g.nx) continue;
+                float gu, gv;
+                if (colin[cc] && rowin) {
+                    gu = hdtdz * w_tdp<FD, false>(wzu, r, cc, i, g.nz) + g.dtdx * a_tdm<FD, false>(ad, cc, j, g.nx, g.nx);
+                    gv = hdtdx * a_tdp<FD, false>(av, cc, j, g.nx) + g.dtdz * w_tdm<FD, false>(wzv, r, cc, i, g.nz, g.nz);
+                } else {
+                    gu = (j >= 1 ? hdtdz * w_tdp<FD, true>(wzu, r, cc, i, g.nz) : 0.f)
+                       + g.dtdx * a_tdm<FD, true>(ad, cc, j, g.nx, g.nx);
+                    gv = (i < g.nz - 1 ? hdtdx * a_tdp<FD, true>(av, cc, j, g.nx) : 0.f)
+                       + (j < g.nx - 1 ? g.dtdz * w_tdm<FD, true>(wzv, r, cc, i, g.nz, g.nz) : 0.f);
+                }
+                np[cc] = p[r][cc] + Bc[r][cc] * gu;
+                nq[cc] = qv[r][cc] + Bc[r][cc] * gv;
+                if (in.want_exact && g.fs && i == 0) {
+                    const int pj = j - g.pad;
+                    if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) {
+                        const float du = in.row0[((long long)s * in.slots + in.slot) * g.nx_dom + pj];
+                        glr[cc] += (double)(g.dtdz * wzv[r + K][cc]) * (double)du * (double)g.dzdx;
+                    }
+                }
+            }
+            if (jb < g.nx) {
+                const long long o = (long long)i * g.P + jb;
+                if (jb + 1 < g.nx) {
+                    *reinterpret_cast<float2 *>(Pp + o) = make_float2(np[0], np[1]);
+                    *reinterpret_cast<float2 *>(Qp + o) = make_float2(nq[0], nq[1]);
+                } else {
+                    Pp[o] = np[0];
+                    Qp[o] = nq[0];
+                }
+            }
+        }
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0 && it + 2 < nsh) {
+            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4);
+            tma_load_4d(S, &tmE, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_EX, s + 2);
+        }
+        const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
+        for (int qq = r0 + tid; qq < r1; qq += NTHR) {
+            const int rid = rv.tile_rec[qq];
+            const long long o = (long long)rv.rz[rid] * g.P + rv.rx[rid];
+            const float *src = in.rec_adj + (long long)s * 4 * g.nt * g.nrec + (long long)n * g.nrec + rid;
+            const float b = m.B[o];
+            atomicAdd(Pp + o, b * src[0]);
+            atomicAdd(Qp + o, b * src[(long long)g.nt * g.nrec]);
+        }
+    }
+    if (in.want_exact && g.fs && c.i0 == 0 && ty == 0) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int j = jb + cc, pj = j - g.pad;
+            if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) in.accLr[(long long)blockIdx.y * g.nx_dom + pj] += glr[cc];
+        }
+    }
+}
+
+// ------------------------------------------------------------- adjoint: strains + gradient
+
+template <int FD, bool EXACT, bool IMG>
+__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+    k4_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
+             AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ)
+{
+    using T = G4<FD, RPT4B>;
+    constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4B;
+    extern __shared__ __align__(128) float sm[];
+    float *aZXZ = sm + 2 * T::S2, *aXXZ = aZXZ + T::S1;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADB);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const int nsh = c.s1 - c.s0;
+    if (nsh <= 0) return;
+    if (tid == 0) {
+        mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
+        fence_async_shared();
+        for (int b = 0; b < 2 && b < nsh; ++b) {
+            mbar_arrive_expect_tx(bar + b, 2 * SN * 4);
+            tma_load_4d(sm + b * T::S2, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+        }
+    }
+    __syncthreads();
+    const bool fix = box_special4(g, c.i0, c.j0, T::TZH, K);
+    const int rd = o.ping, wr = 1 - o.ping;
+    const int jb = c.j0 + 2 * tx;
+    bool colin[2];
+    colin[0] = jb >= T::M && jb <= g.nx - 1 - T::M;
+    colin[1] = jb + 1 >= T::M && jb + 1 <= g.nx - 1 - T::M;
+    float mL2M[RPT][2], mL[RPT][2], mM2[RPT][2], idet[RPT][2], i2m[RPT][2];
+    constexpr int RE = EXACT ? RPT : 1, RI = IMG ? RPT : 1;
+    double gM[RE][2], gL[RE][2], gL2M[RE][2], glam[RI][2], gmu[RI][2];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int i = c.i0 + ty * RPT + r, j = jb + cc;
+            const bool inb = i < g.nz && j < g.nx;
+            const long long off = (long long)i * g.P + j;
+            mL2M[r][cc] = inb ? m.L2M[off] : 0.f;
+            mL[r][cc] = inb ? m.L[off] : 0.f;
+            mM2[r][cc] = inb ? 2.f * m.M[off] : 0.f;
+            idet[r][cc] = inb ? 1.0f / ((mL2M[r][cc] - mL[r][cc]) * (mL2M[r][cc] + mL[r][cc])) : 0.f;
+            i2m[r][cc] = inb ? 1.0f / mM2[r][cc] : 0.f;
+        }
+#pragma unroll
+    for (int r = 0; r < RE; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) gM[r][cc] = gL[r][cc] = gL2M[r][cc] = 0.0;
+#pragma unroll
+    for (int r = 0; r < RI; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) glam[r][cc] = gmu[r][cc] = 0.0;
+
+    for (int it = 0; it < nsh; ++it) {
+        const int s = c.s0 + it;
+        float *S = sm + (it & 1) * T::S2;
+        float *exa = A + ((long long)s * F_N + F_EX) * g.fstride;
+        float *eza = A + ((long long)s * F_N + F_EZ) * g.fstride;
+        float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
+        const float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
+        const float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
+        const float *snap_in = (EXACT && o.slot_in >= 0)
+                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * 3 * g.nd : nullptr;
+        const float *snap_img = (IMG && o.slot_img >= 0)
+                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * 3 * g.nd : nullptr;
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
+            abort3(bar, 2, status);
+            return;
+        }
+        if (fix) {
+            const float *pXX = px_ptr(g, PX, s, PX_NFWD + rd * PXA_N + PXA_XX);
+            const float *pXXZ = px_ptr(g, PX, s, PX_NFWD + rd * PXA_N + PXA_XXZ);
+            const float *pZXZ = pz_ptr(g, PZ, s, PZ_NFWD + rd * PZA_N + PZA_ZXZ);
+            const float *pZZ = pz_ptr(g, PZ, s, PZ_NFWD + rd * PZA_N + PZA_ZZ);
+            float *wXX = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_XX);
+            float *wXXZ = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_XXZ);
+            float *wZXZ = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_ZXZ);
+            float *wZZ = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_ZZ);
+            for (int rr = ty; rr < SH; rr += NWARP) {
+                const int i = c.i0 - K + rr;
+                for (int cc = tx; cc < SW4; cc += TX) {
+                    const int jj = c.j0 - XO4 + cc, q = rr * SW4 + cc;
+                    float pv = 0.f, qq = 0.f;
+                    if (i >= 0 && i < g.nz - 1 && jj >= 1 && jj < g.nx - 1) { pv = S[q]; qq = S[SN + q]; }
+                    float vXX = pv, vZXZ = pv, vXXZ = qq, vZZ = qq;
+                    if (i >= 0 && i < g.nz && jj >= 0 && jj < g.nx) {
+                        const bool own = rr >= K && rr < K + T::TZH && cc >= XO4 && cc < XO4 + TX4;
+                        const int xs = xstrip_index(g, jj), zs = zstrip_index(g, i);
+                        if (xs >= 0) {
+                            const long long px = (long long)i * g.xs_n + xs;
+                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj];
+                            const float p0 = pXX[px], p1 = pXXZ[px];
+                            vXX = (ik + a) * pv + a * p0 / g.dtdx;
+                            vXXZ = (ik + a) * qq + a * p1 / g.dtdx;
+                            if (own) {
+                                wXX[px] = b * (g.dtdx * pv + p0);
+                                wXXZ[px] = b * (g.dtdx * qq + p1);
+                            }
+                        }
+                        if (zs >= 0) {
+                            const long long pz = (long long)zs * g.P + jj;
+                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i];
+                            const float p0 = pZXZ[pz], p1 = pZZ[pz];
+                            vZXZ = (ik + a) * pv + a * p0 / g.dtdz;
+                            vZZ = (ik + a) * qq + a * p1 / g.dtdz;
+                            if (own) {
+                                wZXZ[pz] = b * (g.dtdz * pv + p0);
+                                wZZ[pz] = b * (g.dtdz * qq + p1);
+                            }
+                        }
+                    }
+                    S[q] = vXX; S[SN + q] = vZZ; aZXZ[q] = vZXZ; aXXZ[q] = vXXZ;
+                }
+            }
+            __syncthreads();
+        }
+        const float *aXX = S, *aZZ = S + SN;
+        const float *sZXZ = fix ? aZXZ : S, *sXXZ = fix ? aXXZ : S + SN;
+        float wzz[T::W][2], wzxz[T::W][2];
+        zwin2<T::W, RPT>(wzz, aZZ, ty, tx);
+        zwin2<T::W, RPT>(wzxz, sZXZ, ty, tx);
+        const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = c.i0 + ty * RPT + r;
+            if (i >= g.nz) continue;
+            const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
+            float ea[2] = {0.f, 0.f}, za[2] = {0.f, 0.f}, sa[2] = {0.f, 0.f};
+            if (jb < g.nx) {
+                const long long off = (long long)i * g.P + jb;
+                const float2 a = *reinterpret_cast<const float2 *>(exa + off);
+                const float2 b = *reinterpret_cast<const float2 *>(eza + off);
+                const float2 d = *reinterpret_cast<const float2 *>(esa + off);
+                ea[0] = a.x; ea[1] = a.y; za[0] = b.x; za[1] = b.y; sa[0] = d.x; sa[1] = d.y;
+            }
+            float axx[10], axz[10];
+            xrow(axx, aXX, q);
+            xrow(axz, sXXZ, q);
+            const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
+            float h1[2] = {0.f, 0.f}, h2[2] = {0.f, 0.f}, h3[2] = {0.f, 0.f};
+            if (EXACT && snap_in) {
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int pi = i - g.z0, pj = jb + cc - g.pad;
+                    if (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                        const long long pq = (long long)pi * g.nx_dom + pj;
+                        h1[cc] = __ldcs(snap_in + pq);
+                        h2[cc] = __ldcs(snap_in + g.nd + pq);
+                        h3[cc] = __ldcs(snap_in + 2 * g.nd + pq);
+                    }
+                }
+            }
+            float nex[2], nez[2], nes[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j = jb + cc;
+                nex[cc] = ea[cc]; nez[cc] = za[cc]; nes[cc] = sa[cc];
+                if (j >= g.nx) continue;
+                float sxx = 0.f, szz = 0.f, sxz = 0.f;
+                if (colin[cc] && rowin) {
+                    sxx = g.dtdx * a_tdp<FD, false>(axx, cc, j, g.nx);
+                    szz = g.dtdz * w_tdp<FD, false>(wzz, r, cc, i, g.nz);
+                    sxz = g.dtdz * w_tdm<FD, false>(wzxz, r, cc, i, g.nz, g.nz - 1)
+                        + g.dtdx * a_tdm<FD, false>(axz, cc, j, g.nx, g.nx - 1);
+                } else {
+                    if (i < g.nz - 1) {
+                        sxx = g.dtdx * a_tdp<FD, true>(axx, cc, j, g.nx);
+                        sxz = g.dtdx * a_tdm<FD, true>(axz, cc, j, g.nx, g.nx - 1);
+                    }
+                    if (j >= 1 && j < g.nx - 1) {
+                        szz = g.dtdz * w_tdp<FD, true>(wzz, r, cc, i, g.nz);
+                        sxz += g.dtdz * w_tdm<FD, true>(wzxz, r, cc, i, g.nz, g.nz - 1);
+                        if (g.fs && i == 0) sxz += 2.f * cf<FD>(1) * g.dtdz * wzxz[r + K][cc];
+                    }
+                }
+                const long long off = (long long)i * g.P + j;
+                if (i == ssz && j == ssx) {
+                    const float w = sh.wav[(long long)s * g.nt + n];
+                    if (stype == 0) {
+                        if (o.src_a) o.src_a[(long long)s * g.nt + n] = g.dtdxdz * Qp[off];
+                    } else {
+                        if (o.src_a) o.src_a[(long long)s * g.nt + n] = (g.dt / sh.mcoef[s]) * (ea[cc] + za[cc]);
+                        if (EXACT) {
+                            const double lm = sh.lm[s];
+                            const double glm = -((double)w * g.dt / ((double)sh.mcoef[s] / lm)) / (lm * lm)
+                                               * (double)(ea[cc] + za[cc]);
+                            gM[r % RE][cc] += glm;
+                            gL[r % RE][cc] += glm;
+                        }
+                    }
+                }
+                nex[cc] = ea[cc] + mL2M[r][cc] * sxx + mL[r][cc] * szz;
+                nez[cc] = za[cc] + mL[r][cc] * sxx + mL2M[r][cc] * szz;
+                nes[cc] = sa[cc] + mM2[r][cc] * sxz;
+                if (EXACT) {
+                    const float e1 = (mL2M[r][cc] * h1[cc] - mL[r][cc] * h2[cc]) * idet[r][cc];
+                    const float e2 = (mL2M[r][cc] * h2[cc] - mL[r][cc] * h1[cc]) * idet[r][cc];
+                    const float e3 = h3[cc] * i2m[r][cc];
+                    gL2M[r % RE][cc] += (double)e1 * sxx + (double)e2 * szz;
+                    gL[r % RE][cc] += (double)e2 * sxx + (double)e1 * szz;
+                    gM[r % RE][cc] += 2.0 * (double)e3 * sxz;
+                }
+                const int pi = i - g.z0, pj = j - g.pad;
+                if (IMG && snap_img && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                    const long long pq = (long long)pi * g.nx_dom + pj;
+                    const int ip = (i + 1) % g.nz, im = (i - 1 + g.nz) % g.nz;
+                    const int jp = (j + 1) % g.nx, jm = (j - 1 + g.nx) % g.nx;
+                    const long long oxp = (long long)i * g.P + jp, oxm = (long long)i * g.P + jm;
+                    const long long ozp = (long long)ip * g.P + j, ozm = (long long)im * g.P + j;
+                    const float dxBU = (Pp[oxp] - Pp[oxm]) * g.inv2dx;
+                    const float dzBV = (Qp[ozp] - Qp[ozm]) * g.inv2dz;
+                    const float dzBU = (Pp[ozp] - Pp[ozm]) * g.inv2dz;
+                    const float dxBV = (Qp[oxp] - Qp[oxm]) * g.inv2dx;
+                    const float t1 = snap_img[pq], t2 = snap_img[g.nd + pq], t3 = snap_img[2 * g.nd + pq];
+                    const float e1 = (mL2M[r][cc] * t1 - mL[r][cc] * t2) * idet[r][cc];
+                    const float e2 = (mL2M[r][cc] * t2 - mL[r][cc] * t1) * idet[r][cc];
+                    const float e3 = t3 * i2m[r][cc];
+                    glam[r % RI][cc] -= (double)g.dt * (double)((e1 + e2) * (dxBU + dzBV));
+                    gmu[r % RI][cc] -= (double)g.dt * (double)(2.f * e1 * dxBU + 2.f * e2 * dzBV + e3 * (dzBU + dxBV));
+                }
+            }
+            if (jb < g.nx) {
+                const long long off = (long long)i * g.P + jb;
+                if (jb + 1 < g.nx) {
+                    *reinterpret_cast<float2 *>(exa + off) = make_float2(nex[0], nex[1]);
+                    *reinterpret_cast<float2 *>(eza + off) = make_float2(nez[0], nez[1]);
+                    *reinterpret_cast<float2 *>(esa + off) = make_float2(nes[0], nes[1]);
+                } else {
+                    exa[off] = nex[0]; eza[off] = nez[0]; esa[off] = nes[0];
+                }
+            }
+        }
+        fence_async_shared();
+        __syncthreads();
+        if (tid == 0 && it + 2 < nsh) {
+            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4);
+            tma_load_4d(S, &tmPQ, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
+        }
+        if (n > 0) {
+            const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
+            for (int qq = r0 + tid; qq < r1; qq += NTHR) {
+                const int rid = rv.tile_rec[qq];
+                const long long off = (long long)rv.rz[rid] * g.P + rv.rx[rid];
+                const float *src = o.rec_adj + (long long)s * 4 * g.nt * g.nrec + (long long)(n - 1) * g.nrec + rid;
+                atomicAdd(exa + off, src[2LL * g.nt * g.nrec]);
+                atomicAdd(eza + off, src[3LL * g.nt * g.nrec]);
+            }
+        }
+    }
+    if (EXACT || IMG) {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int i = c.i0 + ty * RPT + r, j = jb + cc;
+                const int pi = i - g.z0, pj = j - g.pad;
+                if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                    double *acc = o.acc + (long long)blockIdx.y * 5 * g.nd + (long long)pi * g.nx_dom + pj;
+                    if (EXACT) {
+                        acc[0] += gM[r % RE][cc];
+                        acc[g.nd] += gL[r % RE][cc];
+                        acc[2 * g.nd] += gL2M[r % RE][cc];
+                    }
+                    if (IMG) {
+                        acc[3 * g.nd] += glam[r % RI][cc];
+                        acc[4 * g.nd] += gmu[r % RI][cc];
+                    }
+                }
+            }
+    }
+}
+
+}  // namespace stfwi

@@ -18,6 +18,7 @@
 #include "../../include/stfwi.h"
 #include "kernels.cuh"
 #include "kernels_v3.cuh"
+#include "kernels_v4.cuh"
 
 using namespace stfwi;
 
@@ -56,8 +57,13 @@ struct stfwi_handle {
     // TMA-pipelined variant: tensor maps and per-kernel shot groups
     int variant = 0, sms = 148;
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
-    int tx3 = 1, tz64 = 1, tz32 = 1;                 // tile counts of the 64- and 32-row tilings
-    int *tile_start64 = nullptr, *tile_rec64 = nullptr;  // receivers grouped by 64-row tiles
+    // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
+    // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
+    // variant 2: 32 x 8*RPT3 and 32 x 32)
+    int tw = TX4, tha = RPT4 * NWARP, thb = RPT4B * NWARP;
+    int ntx = 1, ntza = 1, ntzb = 1;                       // tile counts
+    int *tile_startA = nullptr, *tile_recA = nullptr;      // receivers grouped by the tw x tha tiles
+    int *tile_startB = nullptr, *tile_recB = nullptr;      // receivers grouped by the tw x thb tiles
     int grp[4] = {1, 1, 1, 1}, spgk[4] = {1, 1, 1, 1};
     int acc_groups = 1, acc_used = 1;
     int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
@@ -410,19 +416,37 @@ void launch_fwd_step_plain(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t
 }
 
 template <int FD>
-void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void launch_fwd_step_v3(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
-    if (h->variant == 1) return launch_fwd_step_plain<FD>(h, n, o, st);
-    const int tiles = h->tx3 * h->tz64;
+    const int tiles = h->ntx * h->ntza;
     dim3 block(TX, NWARP);
-    Recv rv64{h->tile_start64, h->tile_rec64, h->rx, h->rz};
+    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     prof_mark(h, 0, n, 0, st);
     k3_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L3<FD>::bytes(L3<FD>::VEL, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->tx3, h->status, h->tmS);
+        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
     k3_fwd_str<FD><<<dim3(tiles, h->grp[1]), block, L3<FD>::bytes(L3<FD>::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), rv64, h->F, h->PX, h->PZ, n, h->spgk[1], h->tx3, o, h->tmV);
+        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV);
+    prof_mark(h, 1, n, 1, st);
+}
+
+template <int FD>
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+{
+    if (h->variant == 1) return launch_fwd_step_plain<FD>(h, n, o, st);
+    if (h->variant == 2) return launch_fwd_step_v3<FD>(h, n, o, st);
+    const int tiles = h->ntx * h->ntza;
+    dim3 block(TX, NWARP);
+    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
+    prof_mark(h, 0, n, 0, st);
+    k4_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L4<FD>::bytes(L4<FD>::VEL, 2), st>>>(
+        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS);
+    prof_mark(h, 0, n, 1, st);
+    prof_mark(h, 1, n, 0, st);
+    auto str = o.energy ? k4_fwd_str<FD, true> : k4_fwd_str<FD, false>;
+    str<<<dim3(tiles, h->grp[1]), block, L4<FD>::bytes(L4<FD>::STR, 2), st>>>(
+        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV);
     prof_mark(h, 1, n, 1, st);
 }
 
@@ -454,25 +478,50 @@ void launch_adj_step_plain(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut
 
 
 template <int FD>
-void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+void launch_adj_step_v3(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
 {
-    if (h->variant == 1) return launch_adj_step_plain<FD>(h, n, ai, ao, st);
     dim3 block(TX, NWARP);
-    Recv rv64{h->tile_start64, h->tile_rec64, h->rx, h->rz};
+    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
+    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
     prof_mark(h, 2, n, 0, st);
-    k3_adj_a<FD><<<dim3(h->tx3 * h->tz64, h->grp[2]), block, L3<FD>::bytes(L3<FD>::ADA, 2), st>>>(
-        h->g, mat_of(h), rv64, h->A, h->PX, h->PZ, n, h->spgk[2], h->tx3, ai, h->status, h->tmE);
+    k3_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L3<FD>::bytes(L3<FD>::ADA, 2), st>>>(
+        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE);
     prof_mark(h, 2, n, 1, st);
     prof_mark(h, 3, n, 0, st);
     auto launch = [&](auto kern) {
-        kern<<<dim3(h->tx3 * h->tz32, h->grp[3]), block, L3<FD>::bytes(L3<FD>::ADB, 2), st>>>(
-            h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spgk[3], h->tx3, ao, h->status,
+        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L3<FD>::bytes(L3<FD>::ADB, 2), st>>>(
+            h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
             h->tmPQ);
     };
     if (ao.want_exact && ao.want_img) launch(k3_adj_b<FD, true, true>);
     else if (ao.want_exact) launch(k3_adj_b<FD, true, false>);
     else if (ao.want_img) launch(k3_adj_b<FD, false, true>);
     else launch(k3_adj_b<FD, false, false>);
+    prof_mark(h, 3, n, 1, st);
+}
+
+template <int FD>
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+{
+    if (h->variant == 1) return launch_adj_step_plain<FD>(h, n, ai, ao, st);
+    if (h->variant == 2) return launch_adj_step_v3<FD>(h, n, ai, ao, st);
+    dim3 block(TX, NWARP);
+    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
+    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
+    prof_mark(h, 2, n, 0, st);
+    k4_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L4<FD>::bytes(L4<FD>::ADA, 2), st>>>(
+        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE);
+    prof_mark(h, 2, n, 1, st);
+    prof_mark(h, 3, n, 0, st);
+    auto launch = [&](auto kern) {
+        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L4<FD>::bytes(L4<FD>::ADB, 2), st>>>(
+            h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
+            h->tmPQ);
+    };
+    if (ao.want_exact && ao.want_img) launch(k4_adj_b<FD, true, true>);
+    else if (ao.want_exact) launch(k4_adj_b<FD, true, false>);
+    else if (ao.want_img) launch(k4_adj_b<FD, false, true>);
+    else launch(k4_adj_b<FD, false, false>);
     prof_mark(h, 3, n, 1, st);
 }
 
@@ -668,13 +717,9 @@ stfwi_status encode(stfwi_handle *h, CUtensorMap *m, void *base, int rank, const
     return STFWI_OK;
 }
 
-template <int FD>
-stfwi_status setup_tma_kernels(stfwi_handle *h)
+template <typename Lk>
+stfwi_status set_smem(stfwi_handle *h, const void *const (&kern)[7])
 {
-    using Lk = L3<FD>;
-    const void *kern[] = {(const void *)k3_fwd_vel<FD>, (const void *)k3_fwd_str<FD>, (const void *)k3_adj_a<FD>,
-                          (const void *)k3_adj_b<FD, true, false>, (const void *)k3_adj_b<FD, true, true>,
-                          (const void *)k3_adj_b<FD, false, true>, (const void *)k3_adj_b<FD, false, false>};
     const size_t bytes[] = {Lk::bytes(Lk::VEL, 2), Lk::bytes(Lk::STR, 2), Lk::bytes(Lk::ADA, 2), Lk::bytes(Lk::ADB, 2),
                             Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2)};
     for (int k = 0; k < 7; ++k) {
@@ -687,6 +732,27 @@ stfwi_status setup_tma_kernels(stfwi_handle *h)
     return STFWI_OK;
 }
 
+template <int FD>
+stfwi_status setup_tma_kernels(stfwi_handle *h)
+{
+    if (h->variant == 2) {
+        const void *const kern[7] = {
+            (const void *)k3_fwd_vel<FD>, (const void *)k3_fwd_str<FD>, (const void *)k3_adj_a<FD>,
+            (const void *)k3_adj_b<FD, true, false>, (const void *)k3_adj_b<FD, true, true>,
+            (const void *)k3_adj_b<FD, false, true>, (const void *)k3_adj_b<FD, false, false>};
+        return set_smem<L3<FD>>(h, kern);
+    }
+    const void *const kern[7] = {
+        (const void *)k4_fwd_vel<FD>, (const void *)k4_fwd_str<FD, false>, (const void *)k4_adj_a<FD>,
+        (const void *)k4_adj_b<FD, true, false>, (const void *)k4_adj_b<FD, true, true>,
+        (const void *)k4_adj_b<FD, false, true>, (const void *)k4_adj_b<FD, false, false>};
+    stfwi_status r = set_smem<L4<FD>>(h, kern);
+    if (r) return r;
+    CK(h, cudaFuncSetAttribute((const void *)k4_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)L4<FD>::bytes(L4<FD>::STR, 2)));
+    return STFWI_OK;
+}
+
 stfwi_status setup_tensor_maps(stfwi_handle *h)
 {
     const Geo &g = h->g;
@@ -694,9 +760,11 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
     const cuuint64_t S = (cuuint64_t)h->d.max_shots;
     const cuuint64_t fdims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.nz, (cuuint64_t)F_N, S};
     const cuuint64_t fstr[3] = {(cuuint64_t)g.P * 4, (cuuint64_t)g.nz * g.P * 4, (cuuint64_t)F_N * g.nz * g.P * 4};
-    const cuuint32_t box3[4] = {(cuuint32_t)SW3, (cuuint32_t)(RPT3 * NWARP + 2 * H), 3, 1};
-    const cuuint32_t box2[4] = {(cuuint32_t)SW3, (cuuint32_t)(RPT3 * NWARP + 2 * H), 2, 1};
-    const cuuint32_t box2s[4] = {(cuuint32_t)SW3, (cuuint32_t)(4 * NWARP + 2 * H), 2, 1};
+    // staged boxes: the tile plus a 4-column and an H-row halo on each side
+    const cuuint32_t bw = (cuuint32_t)(h->tw + 8);
+    const cuuint32_t box3[4] = {bw, (cuuint32_t)(h->tha + 2 * H), 3, 1};
+    const cuuint32_t box2[4] = {bw, (cuuint32_t)(h->tha + 2 * H), 2, 1};
+    const cuuint32_t box2s[4] = {bw, (cuuint32_t)(h->thb + 2 * H), 2, 1};
     stfwi_status r;
     if ((r = encode(h, &h->tmS, h->F, 4, fdims, fstr, box3))) return r;
     if ((r = encode(h, &h->tmV, h->F, 4, fdims, fstr, box2))) return r;
@@ -781,12 +849,17 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
     h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
     h->spg = (d->max_shots + h->groups - 1) / h->groups;
-    h->variant = d->kernel_variant == 1 ? 1 : 0;
-    h->tx3 = (int)((p.nx + TX - 1) / TX);
-    h->tz64 = (int)((p.nz + RPT3 * NWARP - 1) / (RPT3 * NWARP));
-    h->tz32 = (int)((p.nz + 4 * NWARP - 1) / (4 * NWARP));
+    h->variant = (d->kernel_variant == 1 || d->kernel_variant == 2) ? d->kernel_variant : 0;
+    if (h->variant == 2) {
+        h->tw = TX; h->tha = RPT3 * NWARP; h->thb = 4 * NWARP;
+    } else {
+        h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
+    }
+    h->ntx = (int)((p.nx + h->tw - 1) / h->tw);
+    h->ntza = (int)((p.nz + h->tha - 1) / h->tha);
+    h->ntzb = (int)((p.nz + h->thb - 1) / h->thb);
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
-    if (h->variant == 0) {
+    if (h->variant != 1) {
         stfwi_status r = STFWI_OK;
         switch (d->fd_order) {
         case 2: r = setup_tma_kernels<2>(h); break;
@@ -820,8 +893,10 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     ok &= alloc((void **)&h->sx, S * 4) && alloc((void **)&h->sz, S * 4) && alloc((void **)&h->stype, S * 4);
     ok &= alloc((void **)&h->wav, S * d->nt * 4) && alloc((void **)&h->fcoef, S * 4) &&
           alloc((void **)&h->mcoef, S * 4) && alloc((void **)&h->lm, S * 4);
-    ok &= alloc((void **)&h->tile_start64, ((size_t)h->tx3 * h->tz64 + 1) * 4) &&
-          alloc((void **)&h->tile_rec64, nrec * 4);
+    ok &= alloc((void **)&h->tile_startA, ((size_t)h->ntx * h->ntza + 1) * 4) &&
+          alloc((void **)&h->tile_recA, nrec * 4) &&
+          alloc((void **)&h->tile_startB, ((size_t)h->ntx * h->ntzb + 1) * 4) &&
+          alloc((void **)&h->tile_recB, nrec * 4);
     ok &= alloc((void **)&h->tile_start, ((size_t)p.tiles_x * p.tiles_z + 1) * 4) &&
           alloc((void **)&h->tile_rec, nrec * 4) && alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
     ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
@@ -858,7 +933,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     cudaMemset(h->MATS, 0, (size_t)4 * NP * 4);
     cudaMemset(h->F, 0, (size_t)S * F_N * NP * 4);
     cudaMemset(h->A, 0, (size_t)S * F_N * NP * 4);
-    if (h->variant == 0) {
+    if (h->variant != 1) {
         stfwi_status r = setup_tensor_maps(h);
         if (r) {
             fprintf(stderr, "stfwi_create: %s\n", h->err.c_str());
@@ -879,7 +954,7 @@ void stfwi_destroy(stfwi_handle *h)
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
                     h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
-                    h->mis_trace, h->mis_shot, h->src_a, h->tile_start64, h->tile_rec64, h->CKF, h->CKPX,
+                    h->mis_trace, h->mis_shot, h->src_a, h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->CKF, h->CKPX,
                     h->CKPZ};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -943,16 +1018,21 @@ stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *r
     CK(h, cudaMemcpy(h->rz, rz.data(), rz.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->tile_rec, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
-    {   // the same grouping for the 64-row tiles
-        const int nt64 = h->tx3 * h->tz64, TZ64 = RPT3 * NWARP;
-        std::vector<int> c64(nt64 + 1, 0), s64(nt64 + 1, 0), l64(std::max(nrec, 1));
-        for (int r = 0; r < nrec; ++r) c64[(rz[r] / TZ64) * h->tx3 + rx[r] / TX]++;
-        for (int t = 0; t < nt64; ++t) s64[t + 1] = s64[t] + c64[t];
-        std::vector<int> f64(s64.begin(), s64.end() - 1);
-        for (int r = 0; r < nrec; ++r) l64[f64[(rz[r] / TZ64) * h->tx3 + rx[r] / TX]++] = r;
-        CK(h, cudaMemcpy(h->tile_start64, s64.data(), s64.size() * 4, cudaMemcpyHostToDevice));
-        CK(h, cudaMemcpy(h->tile_rec64, l64.data(), l64.size() * 4, cudaMemcpyHostToDevice));
-    }
+    // the same grouping for the two staged tilings
+    auto group = [&](int th, int ntz, int *d_start, int *d_list) -> stfwi_status {
+        const int ntl = h->ntx * ntz;
+        std::vector<int> c(ntl + 1, 0), st(ntl + 1, 0), l(std::max(nrec, 1));
+        for (int r = 0; r < nrec; ++r) c[(rz[r] / th) * h->ntx + rx[r] / h->tw]++;
+        for (int t = 0; t < ntl; ++t) st[t + 1] = st[t] + c[t];
+        std::vector<int> f(st.begin(), st.end() - 1);
+        for (int r = 0; r < nrec; ++r) l[f[(rz[r] / th) * h->ntx + rx[r] / h->tw]++] = r;
+        CK(h, cudaMemcpy(d_start, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(d_list, l.data(), l.size() * 4, cudaMemcpyHostToDevice));
+        return STFWI_OK;
+    };
+    stfwi_status gr;
+    if ((gr = group(h->tha, h->ntza, h->tile_startA, h->tile_recA))) return gr;
+    if ((gr = group(h->thb, h->ntzb, h->tile_startB, h->tile_recB))) return gr;
     h->recv_set = true;
     return STFWI_OK;
 }
@@ -984,7 +1064,7 @@ stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
     h->nshot = nshot;
     g.nshot = nshot;
     h->spg = std::max(1, (nshot + h->groups - 1) / h->groups);
-    if (h->variant == 0) {
+    if (h->variant != 1) {
         const int tiles = g.tiles_x * g.tiles_z;
         for (int k = 0; k < 4; ++k) {
             // two shots per block by default: enough blocks to keep every SM

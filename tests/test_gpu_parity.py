@@ -28,7 +28,7 @@ def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx
                   want_gradient=want_gradient, **kw)
 
 
-VARIANTS = [0, 1]  # TMA-pipelined tiles, plain shared-memory tiles
+VARIANTS = [0, 1, 2]  # two-column TMA tiles (default), plain shared-memory tiles, one-column TMA tiles
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -197,3 +197,63 @@ def test_checkpointed_gradient_equals_store_all(variant):
     for k in (1, 2):
         for a, b in zip(out[k], out[0]):
             assert _rel(a, b) < 1e-12, (k, _rel(a, b))
+
+
+def _smooth_model(nz, nx, seed):
+    """A heterogeneous model with structure at several scales (smoothed noise
+    on a gradient), so that every tile sees different materials."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    zz = np.arange(nz)[:, None] / nz
+    n1 = gaussian_filter(rng.standard_normal((nz, nx)), 4.0)
+    n1 /= np.abs(n1).max()
+    vp = 2200.0 + 900.0 * zz + 250.0 * n1
+    vs = vp / 1.8 + 60.0 * gaussian_filter(rng.standard_normal((nz, nx)), 2.0)
+    rho = 1900.0 + 250.0 * zz + 40.0 * n1
+    return vs, vp, rho
+
+
+@pytest.mark.parametrize("variant", [0, 2])
+@pytest.mark.parametrize("fd,fs", [(8, True), (8, False), (4, True), (2, False)])
+def test_multi_tile_grid_vs_oracle(fd, fs, variant):
+    """A grid of several tiles in x and z (interior tiles without the C-PML
+    fix-up, tile edges inside the stencil reach), with sources and receivers
+    near tile edges: seismograms, misfit and the exact gradient against the
+    FP64 oracle."""
+    nz, nx, pad, nt = 70, 150, 10, 110
+    dx = dz = 10.0
+    dt, fc = 1.0e-3, 18.0
+    vs, vp, rho = _smooth_model(nz, nx, 7)
+    rx = np.arange(0, nx, 3, dtype=np.int32)
+    rz = np.full_like(rx, 0 if fs else 3)
+    rz[::4] = 31                      # a tile-row edge in z (tiles of 16 and 32 rows)
+    sx = np.array([44, 54, 120])      # 44 + pad = 54: two columns below a 64-column tile edge
+    sz = np.array([0 if fs else 5, 22, 47])
+    types = ["force", "moment", "force"]
+    wav = O.ricker(np.arange(nt) * dt, fc, 1.5 / fc) * 1e9
+    geo = dict(rec_x=rx, rec_z=rz, nx_dom=nx, nz_dom=nz, dx=dx, dz=dz, dt=dt, nt=nt, fc=fc, pad=pad,
+               fd_order=fd, free_surface=fs, d0_f32=True)
+    obs = O.forward_batch(vs * 1.02, vp, rho, sx, sz, types, src_wavelet=wav, **geo)[:, 1]
+    ref = O.forward_batch(vs, vp, rho, sx, sz, types, src_wavelet=wav, **geo)
+    kw = dict(src_x=sx, src_z=sz, src_wavelet=wav, observed=obs, src_types=types, component=1,
+              scale=1.0, invert="vs_vp", **geo)
+    (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
+    S = _solver(nt, len(rx), 3, fd, fs, want_gradient=True, pad=pad, nz=nz, nx=nx, dx=dx, dz=dz, dt=dt,
+                fc=fc, kernel_variant=variant)
+    S.set_model(vs, vp, rho)
+    S.set_receivers(rx, rz)
+    S.set_shots(sx, sz, types, wav.astype(np.float32))
+    S.forward(store=True)
+    rec = S.records()
+    for k in range(3):
+        for c in range(4):
+            assert _rel(rec[k, c], ref[k, c]) < 1e-5, (k, c, _rel(rec[k, c], ref[k, c]))
+    mis = S.misfit(obs.astype(np.float32), 1, 1.0)
+    amp = float(np.linalg.norm(rec[:, 1]) / np.linalg.norm(rec[:, 1] - obs))
+    g = S.gradient(exact=True)
+    errs = {"misfit": abs(mis.sum() / loss - 1), "exact_vs": _rel(g["exact"][0], gx_vs),
+            "exact_vp": _rel(g["exact"][1], gx_vp)}
+    print(f"multi-tile fd{fd} fs={fs} variant {variant}: amplification {amp:.1f} errors {errs}")
+    tol = 2e-5 * max(amp, 1.0)
+    assert all(e < tol for e in errs.values()), (tol, errs)
+    S.close()
