@@ -39,8 +39,11 @@ template <int FD> struct L4 {
     using B = G4<FD, RPT4B>;
     static constexpr int VEL = 2 * A::S3;
     static constexpr int STR = 2 * A::S2;
-    static constexpr int ADA = 2 * A::S3 + A::S1;
-    static constexpr int ADB = 2 * B::S2 + 2 * B::S1;
+    // C-PML coefficient tables of a staged box: bx, ax, ikx, Lr per column, bz, az, ikz per row
+    static constexpr int TABA = al32_3(5 * SW4 + 4 * A::SH);
+    static constexpr int TABB = al32_3(5 * SW4 + 4 * B::SH);
+    static constexpr int ADA = 2 * A::S3 + A::S1 + TABA;
+    static constexpr int ADB = 2 * B::S2 + 2 * B::S1 + TABB;
     static constexpr size_t bytes(int floats, int nbar) { return (size_t)floats * 4 + 8 * nbar; }
 };
 
@@ -177,6 +180,62 @@ __device__ __forceinline__ bool box_special4(const Geo &g, int i0, int j0, int t
     return false;
 }
 
+// the strain-phase fix-up only applies C-PML transposes and edge limits, which
+// all lie in the strips: the free-surface row needs none there
+__device__ __forceinline__ bool box_strips4(const Geo &g, int i0, int j0, int tzh, int K)
+{
+    const int r0 = i0 - K, r1 = i0 + tzh + K - 1, c0 = j0 - XO4, c1 = j0 + TX4 + XO4 - 1;
+    if (c0 < g.pad || c1 >= g.nx - g.pad) return true;
+    if (r1 >= g.nz - g.pad) return true;
+    if (!g.fs && r0 < g.pad) return true;
+    return false;
+}
+
+// pml_fwd with the old memory already loaded (the load is issued early)
+__device__ __forceinline__ float pml_fwd_pre(float D, float b, float a, float ik, float old, float *psi)
+{
+    const float pn = b * old + a * D;
+    *psi = pn;
+    return D * ik + pn;
+}
+
+// C-PML coefficients of the box's columns and rows in shared memory (read by
+// the fix-up passes instead of per-cell global loads): per column bx, ax,
+// ikx, Lr (free-surface term) and the x-strip index (-1 outside the strips),
+// per row bz, az, ikz and the z-strip index
+template <int SH>
+__device__ __forceinline__ void pml_table4(const Geo &g, const Mat &m, int i0, int j0, float *tab, int tid)
+{
+    int *itab = reinterpret_cast<int *>(tab);
+    for (int t = tid; t < SW4; t += NTHR) {
+        const int jj = j0 - XO4 + t;
+        const bool in = jj >= 0 && jj < g.nx;
+        const int xs = in ? xstrip_index(g, jj) : -1;
+        tab[t] = xs >= 0 ? m.bx[jj] : 0.f;
+        tab[SW4 + t] = xs >= 0 ? m.ax[jj] : 0.f;
+        tab[2 * SW4 + t] = xs >= 0 ? m.ikx[jj] : 1.f;
+        tab[3 * SW4 + t] = (in && g.fs) ? m.Lr[jj] : 0.f;
+        itab[4 * SW4 + t] = xs;
+    }
+    for (int t = tid; t < SH; t += NTHR) {
+        const int i = i0 + t;
+        const int zs = (i >= 0 && i < g.nz) ? zstrip_index(g, i) : -1;
+        tab[5 * SW4 + t] = zs >= 0 ? m.bz[i] : 0.f;
+        tab[5 * SW4 + SH + t] = zs >= 0 ? m.az[i] : 0.f;
+        tab[5 * SW4 + 2 * SH + t] = zs >= 0 ? m.ikz[i] : 1.f;
+        itab[5 * SW4 + 3 * SH + t] = zs;
+    }
+}
+
+// transposed C-PML on a staged value x with the memory kept in the scaled
+// form phi = psi / (dt / d) of the adjoint step (so the step's factor drops
+// out): returns (1/k + a) x + a phi and stores the new memory b (x + phi)
+__device__ __forceinline__ float pml_adj4(float x, float b, float a, float ik, float phi, float *dst, bool own)
+{
+    if (own) *dst = b * (x + phi);
+    return (ik + a) * x + a * phi;
+}
+
 // ------------------------------------------------------------- forward: velocities
 
 template <int FD>
@@ -246,6 +305,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             return;
         }
         const float *sxx = S, *szz = S + SN, *sxz = S + 2 * SN;
+        float *pSXX = px_ptr(g, PX, s, PX_SXX), *pSXZx = px_ptr(g, PX, s, PX_SXZ);
+        float *pSXZz = pz_ptr(g, PZ, s, PZ_SXZ), *pSZZ = pz_ptr(g, PZ, s, PZ_SZZ);
         float wxz[T::W][2], wzz[T::W][2];
         zwin2<T::W, RPT>(wxz, sxz, ty, tx);
         zwin2<T::W, RPT>(wzz, szz, ty, tx);
@@ -259,6 +320,27 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             xrow(az, sxz, q);
             const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
             const int zs = zstrip_index(g, i);
+            // this row's C-PML memories, requested before the stencils
+            float pxo[2][2] = {{0.f, 0.f}, {0.f, 0.f}}, pzo[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+            float zb = 0.f, za = 0.f, zik = 1.f;
+            if (i < g.nz - 1) {
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int j = jb + cc;
+                    if (j < 1 || j >= g.nx - 1) continue;
+                    if (xs[cc] >= 0) {
+                        const long long px = (long long)i * g.xs_n + xs[cc];
+                        pxo[cc][0] = pSXX[px];
+                        pxo[cc][1] = pSXZx[px];
+                    }
+                    if (zs >= 0) {
+                        const long long pz = (long long)zs * g.P + j;
+                        pzo[cc][0] = pSXZz[pz];
+                        pzo[cc][1] = pSZZ[pz];
+                    }
+                }
+                if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
+            }
             float un[2], vn[2];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
@@ -280,13 +362,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     if (g.fs && i == 0) dzxz = 2.f * cf<FD>(1) * wxz[r + K][cc];
                 }
                 if (xs[cc] >= 0) {
-                    dxx = pml_fwd(dxx, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_SXX) + (long long)i * g.xs_n + xs[cc]);
-                    dxxz = pml_fwd(dxxz, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_SXZ) + (long long)i * g.xs_n + xs[cc]);
+                    const long long px = (long long)i * g.xs_n + xs[cc];
+                    dxx = pml_fwd_pre(dxx, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pSXX + px);
+                    dxxz = pml_fwd_pre(dxxz, bxv[cc], axv[cc], ikxv[cc], pxo[cc][1], pSXZx + px);
                 }
                 if (zs >= 0) {
-                    const float b = m.bz[i], a = m.az[i], ik = m.ikz[i];
-                    dzxz = pml_fwd(dzxz, b, a, ik, pz_ptr(g, PZ, s, PZ_SXZ) + (long long)zs * g.P + j);
-                    dzz = pml_fwd(dzz, b, a, ik, pz_ptr(g, PZ, s, PZ_SZZ) + (long long)zs * g.P + j);
+                    const long long pz = (long long)zs * g.P + j;
+                    dzxz = pml_fwd_pre(dzxz, zb, za, zik, pzo[cc][0], pSXZz + pz);
+                    dzz = pml_fwd_pre(dzz, zb, za, zik, pzo[cc][1], pSZZ + pz);
                 }
                 un[cc] = u[r][cc] + g.dtdx * Bc[r][cc] * dxx + g.dtdz * Bc[r][cc] * dzxz;
                 float vv = v[r][cc] + g.dtdx * Bc[r][cc] * dxxz + g.dtdz * Bc[r][cc] * dzz;
@@ -379,6 +462,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             return;
         }
         const float *sU = S, *sV = S + SN;
+        float *pDXU = px_ptr(g, PX, s, PX_DXU), *pDXV = px_ptr(g, PX, s, PX_DXV);
+        float *pDZV = pz_ptr(g, PZ, s, PZ_DZV), *pDZU = pz_ptr(g, PZ, s, PZ_DZU);
         float wU[T::W][2], wV[T::W][2];
         zwin2<T::W, RPT>(wU, sU, ty, tx);
         zwin2<T::W, RPT>(wV, sV, ty, tx);
@@ -401,6 +486,25 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             xrow(av, sV, q);
             const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
             const int zs = zstrip_index(g, i);
+            // this row's C-PML memories, requested before the stencils
+            float pxo[2][2] = {{0.f, 0.f}, {0.f, 0.f}}, pzo[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+            float zb = 0.f, za = 0.f, zik = 1.f;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int j = jb + cc;
+                if (j >= g.nx) continue;
+                if (xs[cc] >= 0) {
+                    const long long px = (long long)i * g.xs_n + xs[cc];
+                    if (j >= 1) pxo[cc][0] = pDXU[px];
+                    if (i < g.nz - 1) pxo[cc][1] = pDXV[px];
+                }
+                if (zs >= 0) {
+                    const long long pz = (long long)zs * g.P + j;
+                    if (j < g.nx - 1) pzo[cc][0] = pDZV[pz];
+                    if (j >= 1) pzo[cc][1] = pDZU[pz];
+                }
+            }
+            if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
             float nxx[2], nzz[2], nxz[2];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
@@ -419,24 +523,22 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     dzv = w_dm<FD, true>(wV, r, cc, i, g.nz);
                     dzu = w_dp<FD, true>(wU, r, cc, i, g.nz);
                 }
+                const long long px = (long long)i * g.xs_n + xs[cc], pz = (long long)zs * g.P + j;
                 if (j >= 1 && xs[cc] >= 0)
-                    dxu = pml_fwd(dxu, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_DXU) + (long long)i * g.xs_n + xs[cc]);
+                    dxu = pml_fwd_pre(dxu, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pDXU + px);
                 if (j < g.nx - 1) {
                     if (g.fs && i == 0) dzv = Lr0[cc] * dxu * g.dzdx;
-                    if (zs >= 0)
-                        dzv = pml_fwd(dzv, m.bz[i], m.az[i], m.ikz[i], pz_ptr(g, PZ, s, PZ_DZV) + (long long)zs * g.P + j);
+                    if (zs >= 0) dzv = pml_fwd_pre(dzv, zb, za, zik, pzo[cc][0], pDZV + pz);
                 } else {
                     dzv = 0.f;
                 }
                 if (j >= 1) {
-                    if (zs >= 0)
-                        dzu = pml_fwd(dzu, m.bz[i], m.az[i], m.ikz[i], pz_ptr(g, PZ, s, PZ_DZU) + (long long)zs * g.P + j);
+                    if (zs >= 0) dzu = pml_fwd_pre(dzu, zb, za, zik, pzo[cc][1], pDZU + pz);
                 } else {
                     dzu = 0.f;
                 }
                 if (i < g.nz - 1) {
-                    if (xs[cc] >= 0)
-                        dxv = pml_fwd(dxv, bxv[cc], axv[cc], ikxv[cc], px_ptr(g, PX, s, PX_DXV) + (long long)i * g.xs_n + xs[cc]);
+                    if (xs[cc] >= 0) dxv = pml_fwd_pre(dxv, bxv[cc], axv[cc], ikxv[cc], pxo[cc][1], pDXV + px);
                 } else {
                     dxv = 0.f;
                 }
@@ -530,7 +632,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     using T = G4<FD, RPT4>;
     constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4;
     extern __shared__ __align__(128) float sm[];
+    constexpr int NCC = (SW4 + TX - 1) / TX;
     float *aDxV = sm + 2 * T::S3;
+    float *tab = aDxV + T::S1;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADA);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
@@ -546,6 +650,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     }
     __syncthreads();
     const bool fix = box_special4(g, c.i0, c.j0, T::TZH, K);
+    if (fix) pml_table4<SH>(g, m, c.i0 - K, c.j0, tab, tid);   // ordered before use by the first wait's barrier
     const int rd = in.ping, wr = 1 - in.ping;
     const int jb = c.j0 + 2 * tx;
     bool colin[2];
@@ -593,45 +698,63 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             float *wDzV = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_DZV);
             float *wDxU = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_DXU);
             float *wDxV = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_DXV);
+            // box columns [0, xl) and [xr, SW4) lie in the x-strips
+            const int xl = g.pad - (c.j0 - XO4), xr = g.nx - g.pad - (c.j0 - XO4);
+            const float *tbx = tab, *tax = tab + SW4, *tikx = tab + 2 * SW4, *tlr = tab + 3 * SW4;
+            const int *txs = reinterpret_cast<const int *>(tab + 4 * SW4);
+            const float *tbz = tab + 5 * SW4, *taz = tbz + SH, *tikz = taz + SH;
+            const int *tzs = reinterpret_cast<const int *>(tikz + SH);
             for (int rr = ty; rr < SH; rr += NWARP) {
                 const int i = c.i0 - K + rr;
-                for (int cc = tx; cc < SW4; cc += TX) {
+                const int zs = tzs[rr];
+                const bool rowsp = zs >= 0 || (g.fs && i == 0);
+                const bool own_row = rr >= K && rr < K + T::TZH;
+                // the C-PML memories of this row's cells, all requested before any is used
+                float ps[NCC][4];
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
+                    ps[b][0] = ps[b][1] = ps[b][2] = ps[b][3] = 0.f;
+                    if (cc >= SW4) continue;
+                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
+                        const long long pz = (long long)zs * g.P + jj;
+                        ps[b][0] = pDzV[pz];
+                        ps[b][1] = pDzU[pz];
+                    }
+                    const int xs = txs[cc];
+                    if (xs >= 0 && i >= 0 && i < g.nz) {
+                        const long long px = (long long)i * g.xs_n + xs;
+                        ps[b][2] = pDxU[px];
+                        ps[b][3] = pDxV[px];
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX;
+                    if (cc >= SW4) continue;
                     const int jj = c.j0 - XO4 + cc, q = rr * SW4 + cc;
+                    if (!rowsp && cc >= xl && cc < xr) {
+                        // outside the strips and off the free-surface row the
+                        // transform is the identity
+                        aDxV[q] = S[2 * SN + q];
+                        continue;
+                    }
                     const float ea = S[q], za = S[SN + q], sa = S[2 * SN + q];
                     float vDxU = ea, vDzV = za, vDzU = sa, vDxV = sa;
                     if (i >= 0 && i < g.nz && jj >= 0 && jj < g.nx) {
-                        const bool own = rr >= K && rr < K + T::TZH && cc >= XO4 && cc < XO4 + TX4;
-                        const int xs = xstrip_index(g, jj), zs = zstrip_index(g, i);
-                        if (zs >= 0) {
-                            const long long pz = (long long)zs * g.P + jj;
-                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i], ps = pDzV[pz];
-                            vDzV = (ik + a) * za + a * ps / g.dtdz;
-                            if (own) wDzV[pz] = b * (g.dtdz * za + ps);
-                        }
+                        const bool own = own_row && cc >= XO4 && cc < XO4 + TX4;
+                        const int xs = txs[cc];
+                        const long long pz = (long long)zs * g.P + jj, px = (long long)i * g.xs_n + xs;
+                        if (zs >= 0) vDzV = pml_adj4(za, tbz[rr], taz[rr], tikz[rr], ps[b][0], wDzV + pz, own);
                         float din = (jj >= 1) ? ea : 0.f;
-                        if (g.fs && i == 0 && jj < g.nx - 1) din = m.Lr[jj] * vDzV + din;
+                        if (g.fs && i == 0 && jj < g.nx - 1) din = tlr[cc] * vDzV + din;
                         vDxU = din;
-                        if (xs >= 0) {
-                            const long long px = (long long)i * g.xs_n + xs;
-                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj], ps = pDxU[px];
-                            vDxU = (ik + a) * din + a * ps / g.dtdx;
-                            if (own) wDxU[px] = b * (g.dtdx * din + ps);
-                        }
+                        if (xs >= 0) vDxU = pml_adj4(din, tbx[cc], tax[cc], tikx[cc], ps[b][2], wDxU + px, own);
                         const float h = (i < g.nz - 1 && jj < g.nx - 1) ? sa : 0.f;
                         vDzU = h;
                         vDxV = h;
-                        if (zs >= 0) {
-                            const long long pz = (long long)zs * g.P + jj;
-                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i], ps = pDzU[pz];
-                            vDzU = (ik + a) * h + a * ps / hdtdz;
-                            if (own) wDzU[pz] = b * (hdtdz * h + ps);
-                        }
-                        if (xs >= 0) {
-                            const long long px = (long long)i * g.xs_n + xs;
-                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj], ps = pDxV[px];
-                            vDxV = (ik + a) * h + a * ps / hdtdx;
-                            if (own) wDxV[px] = b * (hdtdx * h + ps);
-                        }
+                        if (zs >= 0) vDzU = pml_adj4(h, tbz[rr], taz[rr], tikz[rr], ps[b][1], wDzU + pz, own);
+                        if (xs >= 0) vDxV = pml_adj4(h, tbx[cc], tax[cc], tikx[cc], ps[b][3], wDxV + px, own);
                     }
                     S[q] = vDxU; S[SN + q] = vDzV; S[2 * SN + q] = vDzU; aDxV[q] = vDxV;
                 }
@@ -724,7 +847,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     using T = G4<FD, RPT4B>;
     constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4B;
     extern __shared__ __align__(128) float sm[];
+    constexpr int NCC = (SW4 + TX - 1) / TX;
     float *aZXZ = sm + 2 * T::S2, *aXXZ = aZXZ + T::S1;
+    float *tab = aXXZ + T::S1;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADB);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
@@ -739,7 +864,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         }
     }
     __syncthreads();
-    const bool fix = box_special4(g, c.i0, c.j0, T::TZH, K);
+    const bool fix = box_strips4(g, c.i0, c.j0, T::TZH, K);
+    if (fix) pml_table4<SH>(g, m, c.i0 - K, c.j0, tab, tid);   // ordered before use by the first wait's barrier
     const int rd = o.ping, wr = 1 - o.ping;
     const int jb = c.j0 + 2 * tx;
     bool colin[2];
@@ -795,37 +921,60 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             float *wXXZ = px_ptr(g, PX, s, PX_NFWD + wr * PXA_N + PXA_XXZ);
             float *wZXZ = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_ZXZ);
             float *wZZ = pz_ptr(g, PZ, s, PZ_NFWD + wr * PZA_N + PZA_ZZ);
+            const int xl = g.pad - (c.j0 - XO4), xr = g.nx - g.pad - (c.j0 - XO4);
+            const float *tbx = tab, *tax = tab + SW4, *tikx = tab + 2 * SW4;
+            const int *txs = reinterpret_cast<const int *>(tab + 4 * SW4);
+            const float *tbz = tab + 5 * SW4, *taz = tbz + SH, *tikz = taz + SH;
+            const int *tzs = reinterpret_cast<const int *>(tikz + SH);
             for (int rr = ty; rr < SH; rr += NWARP) {
                 const int i = c.i0 - K + rr;
-                for (int cc = tx; cc < SW4; cc += TX) {
+                const int zs = tzs[rr];
+                const bool rowsp = zs >= 0;
+                const bool own_row = rr >= K && rr < K + T::TZH;
+                float ps[NCC][4];
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
+                    ps[b][0] = ps[b][1] = ps[b][2] = ps[b][3] = 0.f;
+                    if (cc >= SW4) continue;
+                    const int xs = txs[cc];
+                    if (xs >= 0 && i >= 0 && i < g.nz) {
+                        const long long px = (long long)i * g.xs_n + xs;
+                        ps[b][0] = pXX[px];
+                        ps[b][1] = pXXZ[px];
+                    }
+                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
+                        const long long pz = (long long)zs * g.P + jj;
+                        ps[b][2] = pZXZ[pz];
+                        ps[b][3] = pZZ[pz];
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX;
+                    if (cc >= SW4) continue;
                     const int jj = c.j0 - XO4 + cc, q = rr * SW4 + cc;
+                    if (!rowsp && cc >= xl && cc < xr) {
+                        // outside the strips: identity (cells off the grid are
+                        // zero-filled by the tile copy already)
+                        aZXZ[q] = S[q];
+                        aXXZ[q] = S[SN + q];
+                        continue;
+                    }
                     float pv = 0.f, qq = 0.f;
                     if (i >= 0 && i < g.nz - 1 && jj >= 1 && jj < g.nx - 1) { pv = S[q]; qq = S[SN + q]; }
                     float vXX = pv, vZXZ = pv, vXXZ = qq, vZZ = qq;
                     if (i >= 0 && i < g.nz && jj >= 0 && jj < g.nx) {
-                        const bool own = rr >= K && rr < K + T::TZH && cc >= XO4 && cc < XO4 + TX4;
-                        const int xs = xstrip_index(g, jj), zs = zstrip_index(g, i);
+                        const bool own = own_row && cc >= XO4 && cc < XO4 + TX4;
+                        const int xs = txs[cc];
+                        const long long px = (long long)i * g.xs_n + xs, pz = (long long)zs * g.P + jj;
                         if (xs >= 0) {
-                            const long long px = (long long)i * g.xs_n + xs;
-                            const float b = m.bx[jj], a = m.ax[jj], ik = m.ikx[jj];
-                            const float p0 = pXX[px], p1 = pXXZ[px];
-                            vXX = (ik + a) * pv + a * p0 / g.dtdx;
-                            vXXZ = (ik + a) * qq + a * p1 / g.dtdx;
-                            if (own) {
-                                wXX[px] = b * (g.dtdx * pv + p0);
-                                wXXZ[px] = b * (g.dtdx * qq + p1);
-                            }
+                            vXX = pml_adj4(pv, tbx[cc], tax[cc], tikx[cc], ps[b][0], wXX + px, own);
+                            vXXZ = pml_adj4(qq, tbx[cc], tax[cc], tikx[cc], ps[b][1], wXXZ + px, own);
                         }
                         if (zs >= 0) {
-                            const long long pz = (long long)zs * g.P + jj;
-                            const float b = m.bz[i], a = m.az[i], ik = m.ikz[i];
-                            const float p0 = pZXZ[pz], p1 = pZZ[pz];
-                            vZXZ = (ik + a) * pv + a * p0 / g.dtdz;
-                            vZZ = (ik + a) * qq + a * p1 / g.dtdz;
-                            if (own) {
-                                wZXZ[pz] = b * (g.dtdz * pv + p0);
-                                wZZ[pz] = b * (g.dtdz * qq + p1);
-                            }
+                            vZXZ = pml_adj4(pv, tbz[rr], taz[rr], tikz[rr], ps[b][2], wZXZ + pz, own);
+                            vZZ = pml_adj4(qq, tbz[rr], taz[rr], tikz[rr], ps[b][3], wZZ + pz, own);
                         }
                     }
                     S[q] = vXX; S[SN + q] = vZZ; aZXZ[q] = vZXZ; aXXZ[q] = vXXZ;
