@@ -31,14 +31,24 @@ template <int FD, int RPT> struct G4 {
     static constexpr int S1 = al32_3(SN), S2 = al32_3(2 * SN), S3 = al32_3(3 * SN);
 };
 
-constexpr int RPT4 = 4;    // rows per thread: fwd_vel, fwd_str, adj_a
-constexpr int RPT4B = 2;   // rows per thread: adj_b (FP64 sums per cell in registers)
+#ifndef STFWI_V4_RPT
+#define STFWI_V4_RPT 2
+#endif
+#ifndef STFWI_V4_RPTB
+#define STFWI_V4_RPTB 2
+#endif
+constexpr int RPT4 = STFWI_V4_RPT;    // rows per thread: fwd_vel, fwd_str, adj_a
+constexpr int RPT4B = STFWI_V4_RPTB;  // rows per thread: adj_b (FP64 sums per cell in registers)
 
 template <int FD> struct L4 {
     using A = G4<FD, RPT4>;
     using B = G4<FD, RPT4B>;
-    static constexpr int VEL = 2 * A::S3;
-    static constexpr int STR = 2 * A::S2;
+    // own-cell boxes (no halo) staged beside the halo boxes: U, V for the
+    // velocity phase, sxx, szz, sxz for the stress phase
+    static constexpr int OWN2 = al32_3(2 * A::TZH * TX4), OWN3 = al32_3(3 * A::TZH * TX4);
+    static constexpr int VEL_STAGE = A::S3 + OWN2, STR_STAGE = A::S2 + OWN3;
+    static constexpr int VEL = 2 * VEL_STAGE;
+    static constexpr int STR = 2 * STR_STAGE;
     // C-PML coefficient tables of a staged box: bx, ax, ikx, Lr per column, bz, az, ikz per row
     static constexpr int TABA = al32_3(5 * SW4 + 4 * A::SH);
     static constexpr int TABB = al32_3(5 * SW4 + 4 * B::SH);
@@ -241,10 +251,11 @@ __device__ __forceinline__ float pml_adj4(float x, float b, float a, float ik, f
 template <int FD>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_fwd_vel(Geo g, Mat m, Shots sh, float *F, float *PX, float *PZ, int n, int spg, int tiles_x, int *status,
-               const __grid_constant__ CUtensorMap tmS)
+               const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmUo)
 {
     using T = G4<FD, RPT4>;
     constexpr int K = T::K, SN = T::SN, RPT = RPT4;
+    constexpr int STG = L4<FD>::VEL_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::VEL);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -255,8 +266,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
         fence_async_shared();
         for (int b = 0; b < 2 && b < nsh; ++b) {
-            mbar_arrive_expect_tx(bar + b, 3 * SN * 4);
-            tma_load_4d(sm + b * T::S3, &tmS, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+            mbar_arrive_expect_tx(bar + b, 3 * SN * 4 + OWNB);
+            tma_load_4d(sm + b * STG, &tmS, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+            tma_load_4d(sm + b * STG + T::S3, &tmUo, bar + b, c.j0, c.i0, F_U, c.s0 + b);
         }
     }
     __syncthreads();
@@ -284,22 +296,10 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
-        float *S = sm + (it & 1) * T::S3;
+        float *S = sm + (it & 1) * STG;
+        const float *own = S + T::S3;   // [U, V][TZH][TX4] of the tile's own cells
         float *U = F + ((long long)s * F_N + F_U) * g.fstride;
         float *V = F + ((long long)s * F_N + F_V) * g.fstride;
-        float u[RPT][2], v[RPT][2];
-#pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = c.i0 + ty * RPT + r;
-            const long long o = (long long)i * g.P + jb;
-            if (i < g.nz - 1 && jb < g.nx) {
-                const float2 a = *reinterpret_cast<const float2 *>(U + o);
-                const float2 b = *reinterpret_cast<const float2 *>(V + o);
-                u[r][0] = a.x; u[r][1] = a.y; v[r][0] = b.x; v[r][1] = b.y;
-            } else {
-                u[r][0] = u[r][1] = v[r][0] = v[r][1] = 0.f;
-            }
-        }
         if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
             abort3(bar, 2, status);
             return;
@@ -341,12 +341,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
                 if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
             }
+            const float2 u2 = *reinterpret_cast<const float2 *>(own + (ty * RPT + r) * TX4 + 2 * tx);
+            const float2 v2 = *reinterpret_cast<const float2 *>(own + (T::TZH + ty * RPT + r) * TX4 + 2 * tx);
+            const float u[2] = {u2.x, u2.y}, v[2] = {v2.x, v2.y};
             float un[2], vn[2];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
-                un[cc] = u[r][cc];
-                vn[cc] = v[r][cc];
+                un[cc] = u[cc];
+                vn[cc] = v[cc];
                 if (i >= g.nz - 1 || j < 1 || j >= g.nx - 1) continue;
                 float dxx, dzxz, dxxz, dzz;
                 if (colin[cc] && rowin) {
@@ -371,8 +374,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     dzxz = pml_fwd_pre(dzxz, zb, za, zik, pzo[cc][0], pSXZz + pz);
                     dzz = pml_fwd_pre(dzz, zb, za, zik, pzo[cc][1], pSZZ + pz);
                 }
-                un[cc] = u[r][cc] + g.dtdx * Bc[r][cc] * dxx + g.dtdz * Bc[r][cc] * dzxz;
-                float vv = v[r][cc] + g.dtdx * Bc[r][cc] * dxxz + g.dtdz * Bc[r][cc] * dzz;
+                un[cc] = u[cc] + g.dtdx * Bc[r][cc] * dxx + g.dtdz * Bc[r][cc] * dzxz;
+                float vv = v[cc] + g.dtdx * Bc[r][cc] * dxxz + g.dtdz * Bc[r][cc] * dzz;
                 if (stype == 0 && i == ssz && j == ssx) vv = vv + sh.fcoef[s] * sh.wav[(long long)s * g.nt + n];
                 vn[cc] = vv;
             }
@@ -391,8 +394,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
-            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4);
+            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4 + OWNB);
             tma_load_4d(S, &tmS, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_EX, s + 2);
+            tma_load_4d(S + T::S3, &tmUo, bar + (it & 1), c.j0, c.i0, F_U, s + 2);
         }
     }
 }
@@ -402,10 +406,11 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 template <int FD, bool ENERGY>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_fwd_str(Geo g, Mat m, Shots sh, Recv rv, float *F, float *PX, float *PZ, int n, int spg, int tiles_x,
-               FwdOut out, const __grid_constant__ CUtensorMap tmV)
+               FwdOut out, const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmSo)
 {
     using T = G4<FD, RPT4>;
     constexpr int K = T::K, SN = T::SN, RPT = RPT4;
+    constexpr int STG = L4<FD>::STR_STAGE, OWNB = 3 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::STR);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -416,8 +421,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
         fence_async_shared();
         for (int b = 0; b < 2 && b < nsh; ++b) {
-            mbar_arrive_expect_tx(bar + b, 2 * SN * 4);
-            tma_load_4d(sm + b * T::S2, &tmV, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+            mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB);
+            tma_load_4d(sm + b * STG, &tmV, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+            tma_load_4d(sm + b * STG + T::S2, &tmSo, bar + b, c.j0, c.i0, F_EX, c.s0 + b);
         }
     }
     __syncthreads();
@@ -453,7 +459,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
-        float *S = sm + (it & 1) * T::S2;
+        float *S = sm + (it & 1) * STG;
+        const float *own = S + T::S2;   // [sxx, szz, sxz][TZH][TX4] of the tile's own cells
         float *sxx = F + ((long long)s * F_N + F_EX) * g.fstride;
         float *szz = F + ((long long)s * F_N + F_EZ) * g.fstride;
         float *sxz = F + ((long long)s * F_N + F_ES) * g.fstride;
@@ -473,14 +480,11 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int i = c.i0 + ty * RPT + r;
             if (i >= g.nz) continue;
             const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
-            float e1[2] = {0.f, 0.f}, e2[2] = {0.f, 0.f}, e3[2] = {0.f, 0.f};
-            if (jb < g.nx) {
-                const long long o = (long long)i * g.P + jb;
-                const float2 a = *reinterpret_cast<const float2 *>(sxx + o);
-                const float2 b = *reinterpret_cast<const float2 *>(szz + o);
-                const float2 d = *reinterpret_cast<const float2 *>(sxz + o);
-                e1[0] = a.x; e1[1] = a.y; e2[0] = b.x; e2[1] = b.y; e3[0] = d.x; e3[1] = d.y;
-            }
+            const int qo = (ty * RPT + r) * TX4 + 2 * tx;
+            const float2 a2 = *reinterpret_cast<const float2 *>(own + qo);
+            const float2 b2 = *reinterpret_cast<const float2 *>(own + T::TZH * TX4 + qo);
+            const float2 d2 = *reinterpret_cast<const float2 *>(own + 2 * T::TZH * TX4 + qo);
+            const float e1[2] = {a2.x, a2.y}, e2[2] = {b2.x, b2.y}, e3[2] = {d2.x, d2.y};
             float au[10], av[10];
             xrow(au, sU, q);
             xrow(av, sV, q);
@@ -591,8 +595,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
-            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4);
+            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB);
             tma_load_4d(S, &tmV, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
+            tma_load_4d(S + T::S2, &tmSo, bar + (it & 1), c.j0, c.i0, F_EX, s + 2);
         }
         const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
         const float *U = F + ((long long)s * F_N + F_U) * g.fstride;

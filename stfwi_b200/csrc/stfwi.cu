@@ -57,6 +57,7 @@ struct stfwi_handle {
     // TMA-pipelined variant: tensor maps and per-kernel shot groups
     int variant = 0, sms = 148;
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
+    CUtensorMap tmUo{}, tmSo{};    // own-cell boxes of the two-column forward kernels
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
     // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
     // variant 2: 32 x 8*RPT3 and 32 x 32)
@@ -441,12 +442,12 @@ void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     prof_mark(h, 0, n, 0, st);
     k4_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L4<FD>::bytes(L4<FD>::VEL, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS);
+        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
     auto str = o.energy ? k4_fwd_str<FD, true> : k4_fwd_str<FD, false>;
     str<<<dim3(tiles, h->grp[1]), block, L4<FD>::bytes(L4<FD>::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV);
+        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
     prof_mark(h, 1, n, 1, st);
 }
 
@@ -770,6 +771,12 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
     if ((r = encode(h, &h->tmV, h->F, 4, fdims, fstr, box2))) return r;
     if ((r = encode(h, &h->tmE, h->A, 4, fdims, fstr, box3))) return r;
     if ((r = encode(h, &h->tmPQ, h->A, 4, fdims, fstr, box2s))) return r;
+    if (h->variant == 0) {
+        const cuuint32_t own2[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->tha, 2, 1};
+        const cuuint32_t own3[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->tha, 3, 1};
+        if ((r = encode(h, &h->tmUo, h->F, 4, fdims, fstr, own2))) return r;
+        if ((r = encode(h, &h->tmSo, h->F, 4, fdims, fstr, own3))) return r;
+    }
     return STFWI_OK;
 }
 
@@ -1065,11 +1072,13 @@ stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
     g.nshot = nshot;
     h->spg = std::max(1, (nshot + h->groups - 1) / h->groups);
     if (h->variant != 1) {
-        const int tiles = g.tiles_x * g.tiles_z;
+        // shots per block by default (measured on B200, 50 shots of 172 x 540):
+        // enough blocks to keep every SM busy, copies of the next shots in
+        // flight while one computes; the strain phase keeps FP64 sums per cell
+        // over its shots and gains from larger groups
+        static const int dflt4[4] = {3, 3, 3, 4}, dflt3[4] = {2, 2, 2, 2};
         for (int k = 0; k < 4; ++k) {
-            // two shots per block by default: enough blocks to keep every SM
-            // busy, and a second copy in flight while the first computes
-            const int spg = h->d.shot_group > 0 ? h->d.shot_group : 2;
+            const int spg = h->d.shot_group > 0 ? h->d.shot_group : (h->variant == 0 ? dflt4[k] : dflt3[k]);
             int G = (nshot + spg - 1) / spg;
             if (k == 3) G = std::min(G, h->acc_groups);
             h->spgk[k] = (nshot + G - 1) / G;
