@@ -1128,15 +1128,17 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 const int i = c.i0 + ty * RPT + r, j = jb + cc;
                 const int pi = i - g.z0, pj = j - g.pad;
                 if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                    // one block per (tile, shot group) adds to these cells in a
+                    // launch: the atomic adds only avoid waiting for the loads
                     double *acc = o.acc + (long long)blockIdx.y * 5 * g.nd + (long long)pi * g.nx_dom + pj;
                     if (EXACT) {
-                        acc[0] += gM[r % RE][cc];
-                        acc[g.nd] += gL[r % RE][cc];
-                        acc[2 * g.nd] += gL2M[r % RE][cc];
+                        atomicAdd(acc, gM[r % RE][cc]);
+                        atomicAdd(acc + g.nd, gL[r % RE][cc]);
+                        atomicAdd(acc + 2 * g.nd, gL2M[r % RE][cc]);
                     }
                     if (IMG) {
-                        acc[3 * g.nd] += glam[r % RI][cc];
-                        acc[4 * g.nd] += gmu[r % RI][cc];
+                        atomicAdd(acc + 3 * g.nd, glam[r % RI][cc]);
+                        atomicAdd(acc + 4 * g.nd, gmu[r % RI][cc]);
                     }
                 }
             }
