@@ -9,6 +9,8 @@
 // window of RPT + 2K rows.  Halo tiles arrive by TMA (one 4-D bulk tensor
 // copy per shot, double-buffered over the shots a block owns).
 #pragma once
+#include <type_traits>
+
 #include "kernels_v3.cuh"
 
 namespace stfwi {
@@ -190,6 +192,24 @@ __device__ __forceinline__ bool box_special4(const Geo &g, int i0, int j0, int t
     return false;
 }
 
+// do the tile's own cells lie where no slice mask, edge rule, C-PML strip or
+// free-surface row applies (margin M from every edge, outside the strips)?
+// Such tiles take a code path without per-cell guards.
+__device__ __forceinline__ bool tile_plain4(const Geo &g, int i0, int j0, int tzh, int M)
+{
+    const int i1 = i0 + tzh - 1, j1 = j0 + TX4 - 1;
+    if (i0 < M || i1 > g.nz - 1 - M || j0 < M || j1 > g.nx - 1 - M) return false;
+    if (j0 < g.pad || j1 >= g.nx - g.pad) return false;
+    if (i1 >= g.nz - g.pad) return false;
+    if (!g.fs && i0 < g.pad) return false;
+    return true;
+}
+
+__device__ __forceinline__ bool in_tile4(int i, int j, int i0, int j0, int tzh)
+{
+    return i >= i0 && i < i0 + tzh && j >= j0 && j < j0 + TX4;
+}
+
 // the strain-phase fix-up only applies C-PML transposes and edge limits, which
 // all lie in the strips: the free-surface row needs none there
 __device__ __forceinline__ bool box_strips4(const Geo &g, int i0, int j0, int tzh, int K)
@@ -294,6 +314,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             Bc[r][cc] = (i < g.nz && j < g.nx) ? m.B[(long long)i * g.P + j] : 0.f;
         }
 
+    const bool plain = tile_plain4(g, c.i0, c.j0, T::TZH, T::M);
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
         float *S = sm + (it & 1) * STG;
@@ -311,6 +332,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         zwin2<T::W, RPT>(wxz, sxz, ty, tx);
         zwin2<T::W, RPT>(wzz, szz, ty, tx);
         const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+        // LEAN: an interior tile without this shot's source (no per-cell guards)
+        auto rows = [&](auto lean_c) {
+        constexpr bool LEAN = decltype(lean_c)::value;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = c.i0 + ty * RPT + r;
@@ -323,7 +347,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             // this row's C-PML memories, requested before the stencils
             float pxo[2][2] = {{0.f, 0.f}, {0.f, 0.f}}, pzo[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
             float zb = 0.f, za = 0.f, zik = 1.f;
-            if (i < g.nz - 1) {
+            if (!LEAN && i < g.nz - 1) {
 #pragma unroll
                 for (int cc = 0; cc < 2; ++cc) {
                     const int j = jb + cc;
@@ -350,9 +374,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 const int j = jb + cc;
                 un[cc] = u[cc];
                 vn[cc] = v[cc];
-                if (i >= g.nz - 1 || j < 1 || j >= g.nx - 1) continue;
+                if (!LEAN && (i >= g.nz - 1 || j < 1 || j >= g.nx - 1)) continue;
                 float dxx, dzxz, dxxz, dzz;
-                if (colin[cc] && rowin) {
+                if (LEAN || (colin[cc] && rowin)) {
                     dxx = a_dp<FD, false>(ax, cc, j, g.nx);
                     dxxz = a_dm<FD, false>(az, cc, j, g.nx);
                     dzxz = w_dm<FD, false>(wxz, r, cc, i, g.nz);
@@ -364,25 +388,25 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     dzz = w_dp<FD, true>(wzz, r, cc, i, g.nz);
                     if (g.fs && i == 0) dzxz = 2.f * cf<FD>(1) * wxz[r + K][cc];
                 }
-                if (xs[cc] >= 0) {
+                if (!LEAN && xs[cc] >= 0) {
                     const long long px = (long long)i * g.xs_n + xs[cc];
                     dxx = pml_fwd_pre(dxx, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pSXX + px);
                     dxxz = pml_fwd_pre(dxxz, bxv[cc], axv[cc], ikxv[cc], pxo[cc][1], pSXZx + px);
                 }
-                if (zs >= 0) {
+                if (!LEAN && zs >= 0) {
                     const long long pz = (long long)zs * g.P + j;
                     dzxz = pml_fwd_pre(dzxz, zb, za, zik, pzo[cc][0], pSXZz + pz);
                     dzz = pml_fwd_pre(dzz, zb, za, zik, pzo[cc][1], pSZZ + pz);
                 }
                 un[cc] = u[cc] + g.dtdx * Bc[r][cc] * dxx + g.dtdz * Bc[r][cc] * dzxz;
                 float vv = v[cc] + g.dtdx * Bc[r][cc] * dxxz + g.dtdz * Bc[r][cc] * dzz;
-                if (stype == 0 && i == ssz && j == ssx) vv = vv + sh.fcoef[s] * sh.wav[(long long)s * g.nt + n];
+                if (!LEAN && stype == 0 && i == ssz && j == ssx) vv = vv + sh.fcoef[s] * sh.wav[(long long)s * g.nt + n];
                 vn[cc] = vv;
             }
             // cells outside the update region keep their value (column 0, nx-1, row nz-1)
-            if (i < g.nz - 1 && jb < g.nx) {
+            if (LEAN || (i < g.nz - 1 && jb < g.nx)) {
                 const long long o = (long long)i * g.P + jb;
-                if (jb + 1 < g.nx) {
+                if (LEAN || jb + 1 < g.nx) {
                     *reinterpret_cast<float2 *>(U + o) = make_float2(un[0], un[1]);
                     *reinterpret_cast<float2 *>(V + o) = make_float2(vn[0], vn[1]);
                 } else {
@@ -391,6 +415,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
             }
         }
+        };
+        if (plain && !in_tile4(ssz, ssx, c.i0, c.j0, T::TZH)) rows(std::true_type{});
+        else rows(std::false_type{});
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
@@ -457,6 +484,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             if (r < RG) eacc[r][cc] = 0.0;
         }
 
+    const bool plain = tile_plain4(g, c.i0, c.j0, T::TZH, T::M);
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
         float *S = sm + (it & 1) * STG;
@@ -475,10 +503,13 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         zwin2<T::W, RPT>(wU, sU, ty, tx);
         zwin2<T::W, RPT>(wV, sV, ty, tx);
         const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+        // LEAN: an interior tile without this shot's source (no per-cell guards)
+        auto rows = [&](auto lean_c) {
+        constexpr bool LEAN = decltype(lean_c)::value;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = c.i0 + ty * RPT + r;
-            if (i >= g.nz) continue;
+            if (!LEAN && i >= g.nz) continue;
             const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
             const int qo = (ty * RPT + r) * TX4 + 2 * tx;
             const float2 a2 = *reinterpret_cast<const float2 *>(own + qo);
@@ -496,7 +527,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
-                if (j >= g.nx) continue;
+                if (LEAN || j >= g.nx) continue;
                 if (xs[cc] >= 0) {
                     const long long px = (long long)i * g.xs_n + xs[cc];
                     if (j >= 1) pxo[cc][0] = pDXU[px];
@@ -508,15 +539,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     if (j >= 1) pzo[cc][1] = pDZU[pz];
                 }
             }
-            if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
+            if (!LEAN && zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
             float nxx[2], nzz[2], nxz[2];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
                 nxx[cc] = e1[cc]; nzz[cc] = e2[cc]; nxz[cc] = e3[cc];
-                if (j >= g.nx) continue;
+                if (!LEAN && j >= g.nx) continue;
                 float dxu, dzv, dzu, dxv;
-                if (colin[cc] && rowin) {
+                if (LEAN || (colin[cc] && rowin)) {
                     dxu = a_dm<FD, false>(au, cc, j, g.nx);
                     dxv = a_dp<FD, false>(av, cc, j, g.nx);
                     dzv = w_dm<FD, false>(wV, r, cc, i, g.nz);
@@ -528,6 +559,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     dzu = w_dp<FD, true>(wU, r, cc, i, g.nz);
                 }
                 const long long px = (long long)i * g.xs_n + xs[cc], pz = (long long)zs * g.P + j;
+                if (!LEAN) {
                 if (j >= 1 && xs[cc] >= 0)
                     dxu = pml_fwd_pre(dxu, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pDXU + px);
                 if (j < g.nx - 1) {
@@ -546,28 +578,29 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 } else {
                     dxv = 0.f;
                 }
-                const float dex = (j >= 1) ? g.dtdx * dxu : 0.f;
+                }
+                const float dex = (LEAN || j >= 1) ? g.dtdx * dxu : 0.f;
                 const float dez = g.dtdz * dzv;
-                const float des = (i < g.nz - 1 && j < g.nx - 1) ? 0.5f * (g.dtdz * dzu + g.dtdx * dxv) : 0.f;
+                const float des = (LEAN || (i < g.nz - 1 && j < g.nx - 1)) ? 0.5f * (g.dtdz * dzu + g.dtdx * dxv) : 0.f;
                 const float l2m = ml2m[r][cc], l = ml[r][cc];
                 float axx = e1[cc] + l2m * dex + l * dez;
                 float azz = e2[cc] + l * dex + l2m * dez;
                 const float axz = e3[cc] + mm2[r][cc] * des;
-                if (stype == 1 && i == ssz && j == ssx) {
+                if (!LEAN && stype == 1 && i == ssz && j == ssx) {
                     const float stm = sh.wav[(long long)s * g.nt + n] * g.dt / sh.mcoef[s];
                     axx = axx + (l2m + l) * stm;
                     azz = azz + (l + l2m) * stm;
                 }
                 nxx[cc] = axx; nzz[cc] = azz; nxz[cc] = axz;
                 const int pi = i - g.z0, pj = j - g.pad;
-                const bool phys = pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom;
+                const bool phys = LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom);
                 if (out.snap && phys) {
                     float *sp = out.snap + ((long long)s * out.slots + out.slot) * 3 * g.nd + (long long)pi * g.nx_dom + pj;
                     __stcs(sp, axx);
                     __stcs(sp + g.nd, azz);
                     __stcs(sp + 2 * g.nd, axz);
                 }
-                if (out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
+                if (!LEAN && out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
                     out.row0[((long long)s * out.slots + out.slot_row0) * g.nx_dom + pj] = dxu;
                 if (ENERGY) {
                     float f;
@@ -581,9 +614,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     eacc[r % RG][cc] += (double)f * (double)f;
                 }
             }
-            if (jb < g.nx) {
+            if (LEAN || jb < g.nx) {
                 const long long o = (long long)i * g.P + jb;
-                if (jb + 1 < g.nx) {
+                if (LEAN || jb + 1 < g.nx) {
                     *reinterpret_cast<float2 *>(sxx + o) = make_float2(nxx[0], nxx[1]);
                     *reinterpret_cast<float2 *>(szz + o) = make_float2(nzz[0], nzz[1]);
                     *reinterpret_cast<float2 *>(sxz + o) = make_float2(nxz[0], nxz[1]);
@@ -592,6 +625,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
             }
         }
+        };
+        if (plain && !in_tile4(ssz, ssx, c.i0, c.j0, T::TZH)) rows(std::true_type{});
+        else rows(std::false_type{});
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
@@ -655,6 +691,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     }
     __syncthreads();
     const bool fix = box_special4(g, c.i0, c.j0, T::TZH, K);
+    const bool lean = !fix && tile_plain4(g, c.i0, c.j0, T::TZH, T::M);
     if (fix) pml_table4<SH>(g, m, c.i0 - K, c.j0, tab, tid);   // ordered before use by the first wait's barrier
     const int rd = in.ping, wr = 1 - in.ping;
     const int jb = c.j0 + 2 * tx;
@@ -771,10 +808,13 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         float wzu[T::W][2], wzv[T::W][2];
         zwin2<T::W, RPT>(wzu, aDzU, ty, tx);
         zwin2<T::W, RPT>(wzv, aDzV, ty, tx);
+        // LEAN: an interior tile whose box needs no fix-up (no per-cell guards)
+        auto rows = [&](auto lean_c) {
+        constexpr bool LEAN = decltype(lean_c)::value;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = c.i0 + ty * RPT + r;
-            if (i >= g.nz) continue;
+            if (!LEAN && i >= g.nz) continue;
             const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
             float ad[10], av[10];
             xrow(ad, aDxU, q);
@@ -785,9 +825,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
                 np[cc] = p[r][cc]; nq[cc] = qv[r][cc];
-                if (j >= g.nx) continue;
+                if (!LEAN && j >= g.nx) continue;
                 float gu, gv;
-                if (colin[cc] && rowin) {
+                if (LEAN || (colin[cc] && rowin)) {
                     gu = hdtdz * w_tdp<FD, false>(wzu, r, cc, i, g.nz) + g.dtdx * a_tdm<FD, false>(ad, cc, j, g.nx, g.nx);
                     gv = hdtdx * a_tdp<FD, false>(av, cc, j, g.nx) + g.dtdz * w_tdm<FD, false>(wzv, r, cc, i, g.nz, g.nz);
                 } else {
@@ -798,7 +838,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
                 np[cc] = p[r][cc] + Bc[r][cc] * gu;
                 nq[cc] = qv[r][cc] + Bc[r][cc] * gv;
-                if (in.want_exact && g.fs && i == 0) {
+                if (!LEAN && in.want_exact && g.fs && i == 0) {
                     const int pj = j - g.pad;
                     if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) {
                         const float du = in.row0[((long long)s * in.slots + in.slot) * g.nx_dom + pj];
@@ -806,9 +846,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     }
                 }
             }
-            if (jb < g.nx) {
+            if (LEAN || jb < g.nx) {
                 const long long o = (long long)i * g.P + jb;
-                if (jb + 1 < g.nx) {
+                if (LEAN || jb + 1 < g.nx) {
                     *reinterpret_cast<float2 *>(Pp + o) = make_float2(np[0], np[1]);
                     *reinterpret_cast<float2 *>(Qp + o) = make_float2(nq[0], nq[1]);
                 } else {
@@ -817,6 +857,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
             }
         }
+        };
+        if (lean) rows(std::true_type{});
+        else rows(std::false_type{});
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
@@ -870,6 +913,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     }
     __syncthreads();
     const bool fix = box_strips4(g, c.i0, c.j0, T::TZH, K);
+    const bool lean = !fix && tile_plain4(g, c.i0, c.j0, T::TZH, T::M);
     if (fix) pml_table4<SH>(g, m, c.i0 - K, c.j0, tab, tid);   // ordered before use by the first wait's barrier
     const int rd = o.ping, wr = 1 - o.ping;
     const int jb = c.j0 + 2 * tx;
@@ -993,10 +1037,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         zwin2<T::W, RPT>(wzz, aZZ, ty, tx);
         zwin2<T::W, RPT>(wzxz, sZXZ, ty, tx);
         const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
+        // LEAN: an interior tile whose box needs no fix-up, without this
+        // shot's source (no per-cell guards)
+        auto rows = [&](auto lean_c) {
+        constexpr bool LEAN = decltype(lean_c)::value;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = c.i0 + ty * RPT + r;
-            if (i >= g.nz) continue;
+            if (!LEAN && i >= g.nz) continue;
             const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
             float ea[2] = {0.f, 0.f}, za[2] = {0.f, 0.f}, sa[2] = {0.f, 0.f};
             if (jb < g.nx) {
@@ -1015,7 +1063,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 #pragma unroll
                 for (int cc = 0; cc < 2; ++cc) {
                     const int pi = i - g.z0, pj = jb + cc - g.pad;
-                    if (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                    if (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom)) {
                         const long long pq = (long long)pi * g.nx_dom + pj;
                         h1[cc] = __ldcs(snap_in + pq);
                         h2[cc] = __ldcs(snap_in + g.nd + pq);
@@ -1028,9 +1076,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
                 nex[cc] = ea[cc]; nez[cc] = za[cc]; nes[cc] = sa[cc];
-                if (j >= g.nx) continue;
+                if (!LEAN && j >= g.nx) continue;
                 float sxx = 0.f, szz = 0.f, sxz = 0.f;
-                if (colin[cc] && rowin) {
+                if (LEAN || (colin[cc] && rowin)) {
                     sxx = g.dtdx * a_tdp<FD, false>(axx, cc, j, g.nx);
                     szz = g.dtdz * w_tdp<FD, false>(wzz, r, cc, i, g.nz);
                     sxz = g.dtdz * w_tdm<FD, false>(wzxz, r, cc, i, g.nz, g.nz - 1)
@@ -1047,7 +1095,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     }
                 }
                 const long long off = (long long)i * g.P + j;
-                if (i == ssz && j == ssx) {
+                if (!LEAN && i == ssz && j == ssx) {
                     const float w = sh.wav[(long long)s * g.nt + n];
                     if (stype == 0) {
                         if (o.src_a) o.src_a[(long long)s * g.nt + n] = g.dtdxdz * Qp[off];
@@ -1074,7 +1122,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     gM[r % RE][cc] += 2.0 * (double)e3 * sxz;
                 }
                 const int pi = i - g.z0, pj = j - g.pad;
-                if (IMG && snap_img && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                if (IMG && snap_img && (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom))) {
                     const long long pq = (long long)pi * g.nx_dom + pj;
                     const int ip = (i + 1) % g.nz, im = (i - 1 + g.nz) % g.nz;
                     const int jp = (j + 1) % g.nx, jm = (j - 1 + g.nx) % g.nx;
@@ -1092,9 +1140,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     gmu[r % RI][cc] -= (double)g.dt * (double)(2.f * e1 * dxBU + 2.f * e2 * dzBV + e3 * (dzBU + dxBV));
                 }
             }
-            if (jb < g.nx) {
+            if (LEAN || jb < g.nx) {
                 const long long off = (long long)i * g.P + jb;
-                if (jb + 1 < g.nx) {
+                if (LEAN || jb + 1 < g.nx) {
                     *reinterpret_cast<float2 *>(exa + off) = make_float2(nex[0], nex[1]);
                     *reinterpret_cast<float2 *>(eza + off) = make_float2(nez[0], nez[1]);
                     *reinterpret_cast<float2 *>(esa + off) = make_float2(nes[0], nes[1]);
@@ -1103,6 +1151,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 }
             }
         }
+        };
+        if (lean && !in_tile4(ssz, ssx, c.i0, c.j0, T::TZH)) rows(std::true_type{});
+        else rows(std::false_type{});
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {

@@ -227,7 +227,9 @@ def test_multi_tile_grid_vs_oracle(fd, fs, variant):
     rx = np.arange(0, nx, 3, dtype=np.int32)
     rz = np.full_like(rx, 0 if fs else 3)
     rz[::4] = 31                      # a tile-row edge in z (tiles of 16 and 32 rows)
-    sx = np.array([44, 54, 120])      # 44 + pad = 54: two columns below a 64-column tile edge
+    # 44 + pad = 54: two columns below a 64-column tile edge; the second and
+    # third sources sit inside interior tiles (rows 16-31 and 32-47, columns 64-127)
+    sx = np.array([44, 54, 70])
     sz = np.array([0 if fs else 5, 22, 47])
     types = ["force", "moment", "force"]
     wav = O.ricker(np.arange(nt) * dt, fc, 1.5 / fc) * 1e9
