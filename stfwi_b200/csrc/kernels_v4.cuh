@@ -54,7 +54,8 @@ template <int FD> struct L4 {
     // C-PML coefficient tables of a staged box: bx, ax, ikx, Lr per column, bz, az, ikz per row
     static constexpr int TABA = al32_3(5 * SW4 + 4 * A::SH);
     static constexpr int TABB = al32_3(5 * SW4 + 4 * B::SH);
-    static constexpr int ADA = 2 * A::S3 + A::S1 + TABA;
+    static constexpr int ADA_STAGE = A::S3 + OWN2;   // + P, Q of the own cells
+    static constexpr int ADA = 2 * ADA_STAGE + A::S1 + TABA;
     static constexpr int ADB = 2 * B::S2 + 2 * B::S1 + TABB;
     static constexpr size_t bytes(int floats, int nbar) { return (size_t)floats * 4 + 8 * nbar; }
 };
@@ -668,13 +669,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 template <int FD>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_adj_a(Geo g, Mat m, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x, AdjIn in,
-             int *status, const __grid_constant__ CUtensorMap tmE)
+             int *status, const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmPQo)
 {
     using T = G4<FD, RPT4>;
     constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4;
+    constexpr int STG = L4<FD>::ADA_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     constexpr int NCC = (SW4 + TX - 1) / TX;
-    float *aDxV = sm + 2 * T::S3;
+    float *aDxV = sm + 2 * STG;
     float *tab = aDxV + T::S1;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADA);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -685,8 +687,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
         fence_async_shared();
         for (int b = 0; b < 2 && b < nsh; ++b) {
-            mbar_arrive_expect_tx(bar + b, 3 * SN * 4);
-            tma_load_4d(sm + b * T::S3, &tmE, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+            mbar_arrive_expect_tx(bar + b, 3 * SN * 4 + OWNB);
+            tma_load_4d(sm + b * STG, &tmE, bar + b, c.j0 - XO4, c.i0 - K, F_EX, c.s0 + b);
+            tma_load_4d(sm + b * STG + T::S3, &tmPQo, bar + b, c.j0, c.i0, F_U, c.s0 + b);
         }
     }
     __syncthreads();
@@ -711,22 +714,10 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
-        float *S = sm + (it & 1) * T::S3;
+        float *S = sm + (it & 1) * STG;
+        const float *own = S + T::S3;   // [P, Q][TZH][TX4] of the tile's own cells
         float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
         float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
-        float p[RPT][2], qv[RPT][2];
-#pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int i = c.i0 + ty * RPT + r;
-            const long long o = (long long)i * g.P + jb;
-            if (i < g.nz && jb < g.nx) {
-                const float2 a = *reinterpret_cast<const float2 *>(Pp + o);
-                const float2 b = *reinterpret_cast<const float2 *>(Qp + o);
-                p[r][0] = a.x; p[r][1] = a.y; qv[r][0] = b.x; qv[r][1] = b.y;
-            } else {
-                p[r][0] = p[r][1] = qv[r][0] = qv[r][1] = 0.f;
-            }
-        }
         if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
             abort3(bar, 2, status);
             return;
@@ -819,12 +810,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             float ad[10], av[10];
             xrow(ad, aDxU, q);
             xrow(av, aXV, q);
+            const float2 p2 = *reinterpret_cast<const float2 *>(own + (ty * RPT + r) * TX4 + 2 * tx);
+            const float2 q2 = *reinterpret_cast<const float2 *>(own + (T::TZH + ty * RPT + r) * TX4 + 2 * tx);
+            const float pr[2] = {p2.x, p2.y}, qr[2] = {q2.x, q2.y};
             const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
             float np[2], nq[2];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int j = jb + cc;
-                np[cc] = p[r][cc]; nq[cc] = qv[r][cc];
+                np[cc] = pr[cc]; nq[cc] = qr[cc];
                 if (!LEAN && j >= g.nx) continue;
                 float gu, gv;
                 if (LEAN || (colin[cc] && rowin)) {
@@ -836,8 +830,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     gv = (i < g.nz - 1 ? hdtdx * a_tdp<FD, true>(av, cc, j, g.nx) : 0.f)
                        + (j < g.nx - 1 ? g.dtdz * w_tdm<FD, true>(wzv, r, cc, i, g.nz, g.nz) : 0.f);
                 }
-                np[cc] = p[r][cc] + Bc[r][cc] * gu;
-                nq[cc] = qv[r][cc] + Bc[r][cc] * gv;
+                np[cc] = pr[cc] + Bc[r][cc] * gu;
+                nq[cc] = qr[cc] + Bc[r][cc] * gv;
                 if (!LEAN && in.want_exact && g.fs && i == 0) {
                     const int pj = j - g.pad;
                     if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) {
@@ -863,8 +857,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
-            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4);
+            mbar_arrive_expect_tx(bar + (it & 1), 3 * SN * 4 + OWNB);
             tma_load_4d(S, &tmE, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_EX, s + 2);
+            tma_load_4d(S + T::S3, &tmPQo, bar + (it & 1), c.j0, c.i0, F_U, s + 2);
         }
         const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
         for (int qq = r0 + tid; qq < r1; qq += NTHR) {
@@ -922,7 +917,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     colin[1] = jb + 1 >= T::M && jb + 1 <= g.nx - 1 - T::M;
     float mL2M[RPT][2], mL[RPT][2], mM2[RPT][2], idet[RPT][2], i2m[RPT][2];
     constexpr int RE = EXACT ? RPT : 1, RI = IMG ? RPT : 1;
-    double gM[RE][2], gL[RE][2], gL2M[RE][2], glam[RI][2], gmu[RI][2];
+    // per-launch sums over the block's shots (at most a few terms) in FP32;
+    // the sums over steps and shot groups are FP64 (the reductions below)
+    float gM[RE][2], gL[RE][2], gL2M[RE][2], glam[RI][2], gmu[RI][2];
 #pragma unroll
     for (int r = 0; r < RPT; ++r)
 #pragma unroll
@@ -939,11 +936,11 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 #pragma unroll
     for (int r = 0; r < RE; ++r)
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) gM[r][cc] = gL[r][cc] = gL2M[r][cc] = 0.0;
+        for (int cc = 0; cc < 2; ++cc) gM[r][cc] = gL[r][cc] = gL2M[r][cc] = 0.f;
 #pragma unroll
     for (int r = 0; r < RI; ++r)
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) glam[r][cc] = gmu[r][cc] = 0.0;
+        for (int cc = 0; cc < 2; ++cc) glam[r][cc] = gmu[r][cc] = 0.f;
 
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
@@ -1105,8 +1102,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                             const double lm = sh.lm[s];
                             const double glm = -((double)w * g.dt / ((double)sh.mcoef[s] / lm)) / (lm * lm)
                                                * (double)(ea[cc] + za[cc]);
-                            gM[r % RE][cc] += glm;
-                            gL[r % RE][cc] += glm;
+                            gM[r % RE][cc] += (float)glm;
+                            gL[r % RE][cc] += (float)glm;
                         }
                     }
                 }
@@ -1117,9 +1114,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     const float e1 = (mL2M[r][cc] * h1[cc] - mL[r][cc] * h2[cc]) * idet[r][cc];
                     const float e2 = (mL2M[r][cc] * h2[cc] - mL[r][cc] * h1[cc]) * idet[r][cc];
                     const float e3 = h3[cc] * i2m[r][cc];
-                    gL2M[r % RE][cc] += (double)e1 * sxx + (double)e2 * szz;
-                    gL[r % RE][cc] += (double)e2 * sxx + (double)e1 * szz;
-                    gM[r % RE][cc] += 2.0 * (double)e3 * sxz;
+                    gL2M[r % RE][cc] += e1 * sxx + e2 * szz;
+                    gL[r % RE][cc] += e2 * sxx + e1 * szz;
+                    gM[r % RE][cc] += 2.f * e3 * sxz;
                 }
                 const int pi = i - g.z0, pj = j - g.pad;
                 if (IMG && snap_img && (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom))) {
@@ -1136,8 +1133,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     const float e1 = (mL2M[r][cc] * t1 - mL[r][cc] * t2) * idet[r][cc];
                     const float e2 = (mL2M[r][cc] * t2 - mL[r][cc] * t1) * idet[r][cc];
                     const float e3 = t3 * i2m[r][cc];
-                    glam[r % RI][cc] -= (double)g.dt * (double)((e1 + e2) * (dxBU + dzBV));
-                    gmu[r % RI][cc] -= (double)g.dt * (double)(2.f * e1 * dxBU + 2.f * e2 * dzBV + e3 * (dzBU + dxBV));
+                    glam[r % RI][cc] -= g.dt * ((e1 + e2) * (dxBU + dzBV));
+                    gmu[r % RI][cc] -= g.dt * (2.f * e1 * dxBU + 2.f * e2 * dzBV + e3 * (dzBU + dxBV));
                 }
             }
             if (LEAN || jb < g.nx) {
@@ -1183,13 +1180,13 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     // launch: the atomic adds only avoid waiting for the loads
                     double *acc = o.acc + (long long)blockIdx.y * 5 * g.nd + (long long)pi * g.nx_dom + pj;
                     if (EXACT) {
-                        atomicAdd(acc, gM[r % RE][cc]);
-                        atomicAdd(acc + g.nd, gL[r % RE][cc]);
-                        atomicAdd(acc + 2 * g.nd, gL2M[r % RE][cc]);
+                        atomicAdd(acc, (double)gM[r % RE][cc]);
+                        atomicAdd(acc + g.nd, (double)gL[r % RE][cc]);
+                        atomicAdd(acc + 2 * g.nd, (double)gL2M[r % RE][cc]);
                     }
                     if (IMG) {
-                        atomicAdd(acc + 3 * g.nd, glam[r % RI][cc]);
-                        atomicAdd(acc + 4 * g.nd, gmu[r % RI][cc]);
+                        atomicAdd(acc + 3 * g.nd, (double)glam[r % RI][cc]);
+                        atomicAdd(acc + 4 * g.nd, (double)gmu[r % RI][cc]);
                     }
                 }
             }

@@ -57,7 +57,7 @@ struct stfwi_handle {
     // TMA-pipelined variant: tensor maps and per-kernel shot groups
     int variant = 0, sms = 148;
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
-    CUtensorMap tmUo{}, tmSo{};    // own-cell boxes of the two-column forward kernels
+    CUtensorMap tmUo{}, tmSo{}, tmPQo{};   // own-cell boxes of the two-column kernels
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
     // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
     // variant 2: 32 x 8*RPT3 and 32 x 32)
@@ -511,7 +511,7 @@ void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, 
     Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
     prof_mark(h, 2, n, 0, st);
     k4_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L4<FD>::bytes(L4<FD>::ADA, 2), st>>>(
-        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE);
+        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
     prof_mark(h, 2, n, 1, st);
     prof_mark(h, 3, n, 0, st);
     auto launch = [&](auto kern) {
@@ -776,6 +776,7 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
         const cuuint32_t own3[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->tha, 3, 1};
         if ((r = encode(h, &h->tmUo, h->F, 4, fdims, fstr, own2))) return r;
         if ((r = encode(h, &h->tmSo, h->F, 4, fdims, fstr, own3))) return r;
+        if ((r = encode(h, &h->tmPQo, h->A, 4, fdims, fstr, own2))) return r;
     }
     return STFWI_OK;
 }
