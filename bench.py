@@ -333,8 +333,18 @@ def main():
     tot, cnt = ktimes[dom]
     avg_ms = tot / cnt if cnt else float("nan")
     achieved = kb[dom] / (avg_ms * 1e-3) / 1e9 if cnt and avg_ms > 0 else float("nan")
+    # DRAM bytes of one launch of that kernel, from the committed ncu capture of
+    # this workload (per-launch traffic does not depend on the step count)
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic_50shots_fd8.json")) as fh:
+            tr = json.load(fh)
+        if ns == 50 and cfg["fd_order"] == 8:
+            traffic = tr["kernels"][dom]["traffic_bytes"]
+    except (OSError, KeyError, ValueError):
+        pass
     roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None,
+            "frac": achieved / peak, "traffic": traffic,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": kb[dom],
             "kernels_ms_per_launch": {k: (v[0] / max(v[1], 1)) for k, v in ktimes.items()}}
