@@ -59,7 +59,9 @@ typedef struct {
     int32_t max_shots;      /* shot batch capacity */
     double dx, dz, dt;      /* grid spacing [m], time step [s] */
     double fc;              /* source peak frequency, used by the PML profile */
-    int32_t want_gradient;  /* 1: reserve strain history + accumulators */
+    int32_t want_gradient;  /* 1: reserve the stress history + accumulators (g_Vs, g_Vp);
+                               2: also keep the velocities in the history, for the density
+                               gradient g_rho of both modes (kernel_variant 0 only) */
     int32_t shot_group;     /* shots per block (0: automatic) */
     double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
     int32_t kernel_variant; /* 0: two-column TMA-pipelined tiles (default), 1: plain shared-memory tiles,

@@ -168,8 +168,9 @@ def adjoint(Vs, Vp, rho, src_x, src_z, rec_x, rec_z, nx_dom, nz_dom, dx, dz, dt,
 
     ``want`` may hold ``"src"`` (source-wavelet adjoint, (nt,)), ``"gmat"``
     (exact dJ/d(M, L, L2M, B) on the padded grid, [4, nz_t, nx_t]) and
-    ``"img"`` ((g_lam, g_mu) of fwi/imaging.py on the padded grid).  The last
-    two need ``src_wavelet`` to recompute the forward.
+    ``"img"`` ((g_lam, g_mu, g_rho_lame) of fwi/imaging.py on the padded
+    grid; g_rho_lame is the density term of fwi/imaging.py:145-154).  The
+    last two need ``src_wavelet`` to recompute the forward.
     """
     if fd_order not in (2, 4, 8):
         raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
@@ -184,7 +185,7 @@ def adjoint(Vs, Vp, rho, src_x, src_z, rec_x, rec_z, nx_dom, nz_dom, dx, dz, dt,
     ra = np.ascontiguousarray(np.stack([_f64(rec_vx_a), _f64(rec_vz_a), _f64(rec_ex_a), _f64(rec_ez_a)]))
     src_a = np.zeros(nt) if "src" in want else None
     gmat = np.zeros((4, nz, nx)) if "gmat" in want else None
-    img = np.zeros((2, nz, nx)) if "img" in want else None
+    img = np.zeros((3, nz, nx)) if "img" in want else None
     hmask = 0
     hb = {"U_a": 0, "V_a": 1, "ex_a": 2, "ez_a": 3, "es_a": 4}
     for k in hist:
@@ -355,8 +356,8 @@ def gradient_batch(Vs, Vp, rho, src_x, src_z, src_types, rec_x, rec_z, nx_dom, n
                    nt, fc, pad, src_wavelet, rec_adj, fd_order=2, free_surface=True, mode="gmat",
                    ckpt=25, d0_f32=None, precision=64):
     """Per-shot model gradients, OpenMP over shots.  ``mode='gmat'``: exact
-    dJ/d(M, L, L2M, B) [nshot, 4, nz_t, nx_t]; ``mode='img'``: (g_lam, g_mu)
-    of fwi/imaging.py [nshot, 2, nz_t, nx_t]."""
+    dJ/d(M, L, L2M, B) [nshot, 4, nz_t, nx_t]; ``mode='img'``: (g_lam, g_mu,
+    g_rho_lame) of fwi/imaging.py [nshot, 3, nz_t, nx_t]."""
     if d0_f32 is None:
         d0_f32 = np.asarray(Vp).dtype == np.float32
     rec_x, rec_z = _i32(rec_x), _i32(rec_z)
@@ -366,7 +367,7 @@ def gradient_batch(Vs, Vp, rho, src_x, src_z, src_types, rec_x, rec_z, nx_dom, n
     d = make_desc(nz_dom, nx_dom, pad, fd_order, free_surface, nt, rec_x.size, dx, dz, dt, fc, d0_f32)
     nz, nx = grid_shape(nz_dom, nx_dom, pad, free_surface)
     gm = np.zeros((ns, 4, nz, nx)) if mode == "gmat" else None
-    im = np.zeros((ns, 2, nz, nx)) if mode == "img" else None
+    im = np.zeros((ns, 3, nz, nx)) if mode == "img" else None
     fn = getattr(lib(), f"oracle{precision}_gradient_batch")
     rc = fn(ct.byref(d), _dptr(_f64(Vs)), _dptr(_f64(Vp)), _dptr(_f64(rho)), ns, _iptr(src),
             _dptr(_f64(src_wavelet)), _iptr(rec_x), _iptr(rec_z), _dptr(_f64(rec_adj)), _dptr(gm),
@@ -412,7 +413,7 @@ def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observe
     if backend == "ad":
         g_vs, g_vp, g_rho = chain_exact(tot, Vs, Vp, rho)
     else:
-        g_vs, g_vp, g_rho = chain_imaging(tot[0], tot[1], Vs, Vp, rho)
+        g_vs, g_vp, g_rho = chain_imaging(tot[0], tot[1], Vs, Vp, rho, g_rho_lame=tot[2])
     if invert == "vs":
         g_vp = np.zeros_like(g_vp); g_rho = np.zeros_like(g_rho)
     elif invert == "vs_vp":

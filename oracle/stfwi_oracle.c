@@ -798,8 +798,11 @@ int ORACLE(forward)(const oracle_desc *d, const double *vs, const double *vp, co
  * rec_adj   [4][nt][nrec] receiver-data adjoints (vx, vz, ex, ez).
  * src_wav_a [nt] source-wavelet adjoint, optional.
  * gmat      [4][nz][nx] += dJ/d(M, L, L2M, B) on the full grid, optional.
- * img       [2][nz][nx] += (g_lam, g_mu) of fwi/imaging.py on the full grid
- *           (before cropping), optional.
+ * img       [3][nz][nx] += (g_lam, g_mu, g_rho_lame) of fwi/imaging.py on the
+ *           full grid (before cropping), optional; g_rho_lame is the density
+ *           term of fwi/imaging.py:145-154, -dt sum_{n=1}^{nt-2} (vx[n] (U_a[n+1]
+ *           - U_a[n-1]) + vz[n] (V_a[n+1] - V_a[n-1])) / (2 dt), with vx[n] the
+ *           forward velocity after step n and U_a[n] the adjoint carry of step n.
  * hist_mask bits 0..4 (U_a, V_a, ex_a, ez_a, es_a): frames written to
  *           hist_out [nh][nt][nz][nx]; frame it is the carry of adjoint step
  *           it, as adjoint_jax(return_wavefields=...) returns them.
@@ -821,9 +824,14 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
     real **A = carry_alloc(N);
     real *recy = (real *)malloc(sizeof(real) * 4 * (size_t)(nrec ? nrec : 1));
     real **gm = NULL;
-    double *glam = NULL, *gmu = NULL;
+    double *glam = NULL, *gmu = NULL, *grl = NULL;
+    real *vnx = NULL, *vnz = NULL;   /* velocities after the first step of the segment processed before */
     if (gmat) { gm = (real **)malloc(4 * sizeof(real *)); for (int k = 0; k < 4; ++k) gm[k] = zalloc(N); }
-    if (img) { glam = (double *)calloc(N, sizeof(double)); gmu = (double *)calloc(N, sizeof(double)); }
+    if (img) {
+        glam = (double *)calloc(N, sizeof(double)); gmu = (double *)calloc(N, sizeof(double));
+        grl = (double *)calloc(N, sizeof(double));
+        vnx = zalloc(N); vnz = zalloc(N);
+    }
 
     /* forward checkpoints (carry-in of steps 0, ckpt, 2*ckpt, ...) */
     const int nseg = (nt + ckpt - 1) / ckpt;
@@ -872,6 +880,18 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
             if (img) {
                 real **fo = seg[it - t0 + 1]; /* forward carry-out of step it = frame it */
                 imaging_frame(&g, A[C_U], A[C_V], fo[C_EX], fo[C_EZ], fo[C_ES], glam, gmu);
+                /* density term regrouped by adjoint step it: the reference's sum
+                 * over n of vx[n] U_a[n+1] meets this step at n = it-1 (it >= 2),
+                 * its sum of vx[n] U_a[n-1] at n = it+1 (it <= nt-3) */
+                const real *um = seg[it - t0][C_U], *wm = seg[it - t0][C_V];   /* vx, vz after step it-1 */
+                const real *up = (it + 1 < t1) ? seg[it - t0 + 2][C_U] : vnx;    /* after step it+1 */
+                const real *wp = (it + 1 < t1) ? seg[it - t0 + 2][C_V] : vnz;
+                for (size_t q = 0; q < N; ++q) {
+                    double t = 0.0;
+                    if (it >= 2 && it <= nt - 1) t += (double)um[q] * A[C_U][q] + (double)wm[q] * A[C_V][q];
+                    if (it <= nt - 3) t -= (double)up[q] * A[C_U][q] + (double)wp[q] * A[C_V][q];
+                    grl[q] -= 0.5 * t;
+                }
             }
             if (hist_out) {
                 int kh = 0;
@@ -883,13 +903,17 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
                     }
             }
         }
+        if (img && need_fwd) {   /* velocities after step t0, for step t0 - 1 of the next (earlier) segment */
+            memcpy(vnx, seg[1][C_U], N * sizeof(real));
+            memcpy(vnz, seg[1][C_V], N * sizeof(real));
+        }
     }
 
     if (gmat)
         for (int k = 0; k < 4; ++k)
             for (size_t q = 0; q < N; ++q) gmat[k * N + q] += (double)gm[k][q];
     if (img)
-        for (size_t q = 0; q < N; ++q) { img[q] += glam[q]; img[N + q] += gmu[q]; }
+        for (size_t q = 0; q < N; ++q) { img[q] += glam[q]; img[N + q] += gmu[q]; img[2 * N + q] += grl[q]; }
 
     if (need_fwd) {
         for (int k = 0; k < nseg; ++k) carry_free(ck[k]);
@@ -901,7 +925,7 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
         carry_free(tmp);
     }
     if (gm) { for (int k = 0; k < 4; ++k) free(gm[k]); free(gm); }
-    free(glam); free(gmu);
+    free(glam); free(gmu); free(grl); free(vnx); free(vnz);
     free(recy);
     carry_free(A);
     grid_free(&g);
@@ -943,7 +967,7 @@ int ORACLE(gradient_batch)(const oracle_desc *d, const double *vs, const double 
         int rc = ORACLE(adjoint)(d, vs, vp, rho, src[3 * s], src[3 * s + 1], src[3 * s + 2], wavelet,
                                  rec_x, rec_z, rec_adj + (size_t)s * 4 * d->nt * d->nrec, NULL,
                                  gmat_out ? gmat_out + (size_t)s * 4 * N : NULL,
-                                 img_out ? img_out + (size_t)s * 2 * N : NULL, 0, NULL, ckpt);
+                                 img_out ? img_out + (size_t)s * 3 * N : NULL, 0, NULL, ckpt);
         if (rc) bad |= 1;
     }
     return bad ? -1 : 0;

@@ -58,6 +58,7 @@ struct Geo {
     long long xstride;         // nz*xs_n  (one x-psi array)
     long long zstride;         // zs_n*P   (one z-psi array)
     long long nd;              // nz_dom*nx_dom
+    int snf;                   // history fields per slot: 3 (stresses) or 5 (+ U, V)
 };
 
 struct Mat {
@@ -230,7 +231,7 @@ __global__ void __launch_bounds__(NTHR) k_fwd_vel(Geo g, Mat m, Shots sh, float 
 
 struct FwdOut {
     float *rec;          // [nshot][4][nt][nrec]
-    float *snap;         // strain history: + (s*slots + slot)*3*nd, or null
+    float *snap;         // history: + (s*slots + slot)*snf*nd, or null
     float *row0;         // post-PML d(vx)/dx at row 0 (free surface): + (s*slots+slot_row0)*nx_dom, or null
     int slots, slot;     // history slot written by this step (its carry-out)
     int slot_row0;       // row-0 slot of this step
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(NTHR) k_fwd_str(Geo g, Mat m, Shots sh, Recv r
             const int pi = i - g.z0, pj = j - g.pad;
             const bool phys = pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom;
             if (out.snap && phys) {
-                float *sp = out.snap + ((long long)s * out.slots + out.slot) * 3 * g.nd + (long long)pi * g.nx_dom + pj;
+                float *sp = out.snap + ((long long)s * out.slots + out.slot) * g.snf * g.nd + (long long)pi * g.nx_dom + pj;
                 __stcs(sp, exn);
                 __stcs(sp + g.nd, ezn);
                 __stcs(sp + 2 * g.nd, esn);
@@ -520,11 +521,13 @@ __global__ void __launch_bounds__(NTHR) k_adj_a(Geo g, Mat m, Recv rv, float *A,
 // ---------------------------------------------------------------- adjoint: strains + gradient
 
 struct AdjOut {
-    const float *snap;     // strain history base (s*slots + slot)*3*nd
+    const float *snap;     // history base (s*slots + slot)*snf*nd
     int slots;
     int slot_in;           // slot of the forward carry-in of this step (-1: zero state)
     int slot_img;          // slot of the forward carry-out of this step (imaging), -1 if none
-    double *acc;           // [groups][5][nd]: gM, gL, gL2M (exact), glam, gmu (imaging)
+    int slot_next;         // slot of the carry-out of the next step (density imaging term), -1 if none
+    int accp;              // accumulator planes per group (5, or 7 with the density terms)
+    double *acc;           // [groups][accp][nd]: gM, gL, gL2M (exact), glam, gmu (imaging), gB (exact), g_rho_lame (imaging)
     int want_exact, want_img;
     float *src_a;          // [nshot][nt] or null
     const float *rec_adj;  // [nshot][4][nt][nrec]
@@ -618,9 +621,9 @@ __global__ void __launch_bounds__(NTHR) k_adj_b(Geo g, Mat m, Shots sh, Recv rv,
         float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
         const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
         const float *snap_in = (EXACT && o.slot_in >= 0)
-                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * 3 * g.nd : nullptr;
+                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * g.snf * g.nd : nullptr;
         const float *snap_img = (IMG && o.slot_img >= 0)
-                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * 3 * g.nd : nullptr;
+                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * g.snf * g.nd : nullptr;
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
             const int i = i0 + ty * RPT + r;
@@ -719,7 +722,7 @@ __global__ void __launch_bounds__(NTHR) k_adj_b(Geo g, Mat m, Shots sh, Recv rv,
             const int i = i0 + ty * RPT + r;
             const int pi = i - g.z0, pj = j - g.pad;
             if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
-                double *acc = o.acc + (long long)grp * 5 * g.nd + (long long)pi * g.nx_dom + pj;
+                double *acc = o.acc + (long long)grp * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
                 if (EXACT) {
                     acc[0] += gM[r % RE];
                     acc[g.nd] += gL[r % RE];

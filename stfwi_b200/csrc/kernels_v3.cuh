@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V3_MINBLOCKS_HEAVY)
             const int pi = i - g.z0, pj = j - g.pad;
             const bool phys = pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom;
             if (out.snap && phys) {
-                float *sp = out.snap + ((long long)s * out.slots + out.slot) * 3 * g.nd + (long long)pi * g.nx_dom + pj;
+                float *sp = out.snap + ((long long)s * out.slots + out.slot) * g.snf * g.nd + (long long)pi * g.nx_dom + pj;
                 __stcs(sp, axx);
                 __stcs(sp + g.nd, azz);
                 __stcs(sp + 2 * g.nd, axz);
@@ -705,9 +705,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V3_MINBLOCKS_HEAVY)
         const float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
         const float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
         const float *snap_in = (EXACT && o.slot_in >= 0)
-                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * 3 * g.nd : nullptr;
+                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * g.snf * g.nd : nullptr;
         const float *snap_img = (IMG && o.slot_img >= 0)
-                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * 3 * g.nd : nullptr;
+                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * g.snf * g.nd : nullptr;
         float ea[RPT], za[RPT], sa[RPT], h1[RPT], h2[RPT], h3[RPT];
 #pragma unroll
         for (int r = 0; r < RPT; ++r) {
@@ -877,7 +877,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V3_MINBLOCKS_HEAVY)
             const int i = c.i0 + ty * RPT + r;
             const int pi = i - g.z0, pj = j - g.pad;
             if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
-                double *acc = o.acc + (long long)blockIdx.y * 5 * g.nd + (long long)pi * g.nx_dom + pj;
+                double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
                 if (EXACT) {
                     acc[0] += gM[r % RE];
                     acc[g.nd] += gL[r % RE];

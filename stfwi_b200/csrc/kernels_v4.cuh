@@ -596,10 +596,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 const int pi = i - g.z0, pj = j - g.pad;
                 const bool phys = LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom);
                 if (out.snap && phys) {
-                    float *sp = out.snap + ((long long)s * out.slots + out.slot) * 3 * g.nd + (long long)pi * g.nx_dom + pj;
+                    float *sp = out.snap + ((long long)s * out.slots + out.slot) * g.snf * g.nd + (long long)pi * g.nx_dom + pj;
                     __stcs(sp, axx);
                     __stcs(sp + g.nd, azz);
                     __stcs(sp + 2 * g.nd, axz);
+                    if (g.snf == 5) {   // velocities of this step (density gradient)
+                        __stcs(sp + 3 * g.nd, au[4 + cc]);
+                        __stcs(sp + 4 * g.nd, av[4 + cc]);
+                    }
                 }
                 if (!LEAN && out.row0 && g.fs && i == 0 && pj >= 0 && pj < g.nx_dom)
                     out.row0[((long long)s * out.slots + out.slot_row0) * g.nx_dom + pj] = dxu;
@@ -882,7 +886,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 // ------------------------------------------------------------- adjoint: strains + gradient
 
-template <int FD, bool EXACT, bool IMG>
+template <int FD, bool EXACT, bool IMG, bool RHO>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
              AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ)
@@ -920,6 +924,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     // per-launch sums over the block's shots (at most a few terms) in FP32;
     // the sums over steps and shot groups are FP64 (the reductions below)
     float gM[RE][2], gL[RE][2], gL2M[RE][2], glam[RI][2], gmu[RI][2];
+    // density terms (history with velocities): dJ/dB of the exact gradient
+    // and the rho term of the imaging formula
+    constexpr int RB = (EXACT && RHO) ? RPT : 1, RR = (IMG && RHO) ? RPT : 1;
+    float gB[RB][2], grl[RR][2];
+#pragma unroll
+    for (int r = 0; r < RB; ++r) gB[r][0] = gB[r][1] = 0.f;
+#pragma unroll
+    for (int r = 0; r < RR; ++r) grl[r][0] = grl[r][1] = 0.f;
 #pragma unroll
     for (int r = 0; r < RPT; ++r)
 #pragma unroll
@@ -951,9 +963,11 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         const float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
         const float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
         const float *snap_in = (EXACT && o.slot_in >= 0)
-                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * 3 * g.nd : nullptr;
-        const float *snap_img = (IMG && o.slot_img >= 0)
-                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * 3 * g.nd : nullptr;
+                                   ? o.snap + ((long long)s * o.slots + o.slot_in) * g.snf * g.nd : nullptr;
+        const float *snap_img = ((IMG || RHO) && o.slot_img >= 0)
+                                    ? o.snap + ((long long)s * o.slots + o.slot_img) * g.snf * g.nd : nullptr;
+        const float *snap_next = (IMG && RHO && o.slot_next >= 0)
+                                     ? o.snap + ((long long)s * o.slots + o.slot_next) * g.snf * g.nd : nullptr;
         if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
             abort3(bar, 2, status);
             return;
@@ -1119,6 +1133,27 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     gM[r % RE][cc] += 2.f * e3 * sxz;
                 }
                 const int pi = i - g.z0, pj = j - g.pad;
+                if (RHO && (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom))) {
+                    const long long pq = (long long)pi * g.nx_dom + pj;
+                    const float pc = Pp[off], qc = Qp[off], bb = m.B[off];
+                    if (EXACT && snap_in && snap_img) {
+                        // dJ/dB: U_a dU/B + V_a dV/B with U_a = P/B and the
+                        // step's velocity increments from the history
+                        const float du = snap_img[3 * g.nd + pq] - snap_in[3 * g.nd + pq];
+                        const float dv = snap_img[4 * g.nd + pq] - snap_in[4 * g.nd + pq];
+                        gB[r % RB][cc] += (pc * du + qc * dv) / (bb * bb);
+                    }
+                    if (IMG) {
+                        // -1/2 U_a(n) (vx(n-1) - vx(n+1)), the rho term of the
+                        // imaging formula regrouped by adjoint step
+                        const float ua = pc / bb, va = qc / bb;
+                        float t = 0.f;
+                        if (n >= 2 && snap_in) t += ua * snap_in[3 * g.nd + pq] + va * snap_in[4 * g.nd + pq];
+                        if (n <= g.nt - 3 && snap_next)
+                            t -= ua * snap_next[3 * g.nd + pq] + va * snap_next[4 * g.nd + pq];
+                        grl[r % RR][cc] -= 0.5f * t;
+                    }
+                }
                 if (IMG && snap_img && (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom))) {
                     const long long pq = (long long)pi * g.nx_dom + pj;
                     const int ip = (i + 1) % g.nz, im = (i - 1 + g.nz) % g.nz;
@@ -1178,7 +1213,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
                     // one block per (tile, shot group) adds to these cells in a
                     // launch: the atomic adds only avoid waiting for the loads
-                    double *acc = o.acc + (long long)blockIdx.y * 5 * g.nd + (long long)pi * g.nx_dom + pj;
+                    double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
                     if (EXACT) {
                         atomicAdd(acc, (double)gM[r % RE][cc]);
                         atomicAdd(acc + g.nd, (double)gL[r % RE][cc]);
@@ -1188,6 +1223,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                         atomicAdd(acc + 3 * g.nd, (double)glam[r % RI][cc]);
                         atomicAdd(acc + 4 * g.nd, (double)gmu[r % RI][cc]);
                     }
+                    if (EXACT && RHO) atomicAdd(acc + 5 * g.nd, (double)gB[r % RB][cc]);
+                    if (IMG && RHO) atomicAdd(acc + 6 * g.nd, (double)grl[r % RR][cc]);
                 }
             }
     }

@@ -56,6 +56,7 @@ struct stfwi_handle {
     bool model_set = false;
     // TMA-pipelined variant: tensor maps and per-kernel shot groups
     int variant = 0, sms = 148;
+    int accp = 5;   // accumulator planes per shot group (7 with the density terms)
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
     CUtensorMap tmUo{}, tmSo{}, tmPQo{};   // own-cell boxes of the two-column kernels
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
@@ -161,11 +162,16 @@ Plan make_plan(const stfwi_desc *d, int k)
     const int G = auto_groups(d, p.tiles_x * p.tiles_z);
     p.fields = (size_t)2 * S * F_N * p.nz * p.P * sizeof(float);
     p.psi = (size_t)S * (NPX * p.nz * p.xs_n + NPZ * p.zs_n * p.P) * sizeof(float);
-    p.snap = d->want_gradient ? (size_t)S * (k + 1) * 3 * p.nd * sizeof(float) : 0;
-    p.row0 = (d->want_gradient && d->free_surface) ? (size_t)S * (k + 1) * d->nx_dom * sizeof(float) : 0;
+    // history fields per slot: the stresses, plus U and V for the density
+    // gradient (want_gradient == 2); with checkpoints and velocities one more
+    // slot holds the first output of the following segment
+    const int snf = d->want_gradient == 2 ? 5 : 3;
+    const int slots = k + 1 + ((snf == 5 && k < d->nt) ? 1 : 0);
+    p.snap = d->want_gradient ? (size_t)S * slots * snf * p.nd * sizeof(float) : 0;
+    p.row0 = (d->want_gradient && d->free_surface) ? (size_t)S * slots * d->nx_dom * sizeof(float) : 0;
     const long long ncp = (d->want_gradient && k < d->nt) ? (d->nt + k - 1) / k : 0;
     p.ckpt = (size_t)ncp * S * (F_N * p.nz * p.P + PX_NFWD * p.nz * p.xs_n + PZ_NFWD * p.zs_n * p.P) * sizeof(float);
-    p.acc = (size_t)G * (5 * p.nd + d->nx_dom) * sizeof(double) + 3 * p.nd * 2 * sizeof(double);
+    p.acc = (size_t)G * ((snf == 5 ? 7 : 5) * p.nd + d->nx_dom) * sizeof(double) + 3 * p.nd * 2 * sizeof(double);
     p.rec = (size_t)2 * S * 4 * d->nt * std::max(d->nrec, 1) * sizeof(float)
           + (size_t)S * d->nt * std::max(d->nrec, 1) * sizeof(float);
     p.misc = (size_t)(8 * p.nz * p.P + 4 * p.nd) * sizeof(float) + (size_t)p.nz * p.nx * sizeof(double)
@@ -346,7 +352,7 @@ __global__ void k_misfit_reduce(int nshot, int nrec, const double *mis_trace, do
 // physical grid.  EXACT: M = rho Vs^2, L2M = rho Vp^2, L = L2M - 2M; the
 // free-surface ratio Lr = -L/L2M contributes on row 0.  IMAGING:
 // fwi/imaging.py:165-167.
-__global__ void k_finalize(Geo g, int groups, int lr_rows, const double *acc, const double *accLr,
+__global__ void k_finalize(Geo g, int groups, int accp, int lr_rows, const double *acc, const double *accLr,
                            const float *L2M, const float *L, const float *vs, const float *vp,
                            const float *rho, int want_exact, int want_img, double *out_exact,
                            double *out_img)
@@ -354,10 +360,11 @@ __global__ void k_finalize(Geo g, int groups, int lr_rows, const double *acc, co
     const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (q >= g.nd) return;
     const int pi = (int)(q / g.nx_dom), pj = (int)(q % g.nx_dom);
-    double gM = 0, gL = 0, gL2M = 0, gla = 0, gmu = 0;
+    double gM = 0, gL = 0, gL2M = 0, gla = 0, gmu = 0, gB = 0, grl = 0;
     for (int k = 0; k < groups; ++k) {
-        const double *a = acc + (long long)k * 5 * g.nd + q;
+        const double *a = acc + (long long)k * accp * g.nd + q;
         gM += a[0]; gL += a[g.nd]; gL2M += a[2 * g.nd]; gla += a[3 * g.nd]; gmu += a[4 * g.nd];
+        if (accp == 7) { gB += a[5 * g.nd]; grl += a[6 * g.nd]; }
     }
     const double r = rho[q], a = vs[q], b = vp[q];
     if (want_exact) {
@@ -371,12 +378,13 @@ __global__ void k_finalize(Geo g, int groups, int lr_rows, const double *acc, co
         }
         out_exact[q] = 2.0 * r * a * (gM - 2.0 * gL);
         out_exact[g.nd + q] = 2.0 * r * b * (gL2M + gL);
-        out_exact[2 * g.nd + q] = 0.0;
+        // M = rho Vs^2, L2M = rho Vp^2, L = rho (Vp^2 - 2 Vs^2), B = 1/rho
+        out_exact[2 * g.nd + q] = accp == 7 ? a * a * gM + b * b * gL2M + (b * b - 2.0 * a * a) * gL - gB / (r * r) : 0.0;
     }
     if (want_img) {
         out_img[q] = 2.0 * r * a * (gmu - 2.0 * gla);
         out_img[g.nd + q] = 2.0 * r * b * gla;
-        out_img[2 * g.nd + q] = (b * b - 2.0 * a * a) * gla + a * a * gmu;
+        out_img[2 * g.nd + q] = (b * b - 2.0 * a * a) * gla + a * a * gmu + grl;
     }
 }
 
@@ -519,10 +527,11 @@ void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, 
             h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
             h->tmPQ);
     };
-    if (ao.want_exact && ao.want_img) launch(k4_adj_b<FD, true, true>);
-    else if (ao.want_exact) launch(k4_adj_b<FD, true, false>);
-    else if (ao.want_img) launch(k4_adj_b<FD, false, true>);
-    else launch(k4_adj_b<FD, false, false>);
+    const bool rho = h->g.snf == 5;
+    if (ao.want_exact && ao.want_img) rho ? launch(k4_adj_b<FD, true, true, true>) : launch(k4_adj_b<FD, true, true, false>);
+    else if (ao.want_exact) rho ? launch(k4_adj_b<FD, true, false, true>) : launch(k4_adj_b<FD, true, false, false>);
+    else if (ao.want_img) rho ? launch(k4_adj_b<FD, false, true, true>) : launch(k4_adj_b<FD, false, true, false>);
+    else launch(k4_adj_b<FD, false, false, false>);
     prof_mark(h, 3, n, 1, st);
 }
 
@@ -550,7 +559,7 @@ stfwi_status zero_adjoint_state(stfwi_handle *h, cudaStream_t st)
         CK(h, cudaMemsetAsync(h->PZ + ((long long)s * NPZ + PZ_NFWD) * g.zstride, 0,
                               (size_t)2 * PZA_N * g.zstride * sizeof(float), st));
     }
-    CK(h, cudaMemsetAsync(h->acc, 0, (size_t)h->acc_used * 5 * g.nd * sizeof(double), st));
+    CK(h, cudaMemsetAsync(h->acc, 0, (size_t)h->acc_used * h->accp * g.nd * sizeof(double), st));
     CK(h, cudaMemsetAsync(h->accLr, 0, (size_t)h->lr_used * g.nx_dom * sizeof(double), st));
     return STFWI_OK;
 }
@@ -564,9 +573,13 @@ __global__ void k_snap_state(Geo g, int slots, const float *F, float *snap)
     if (q >= g.nd) return;
     const int pi = (int)(q / g.nx_dom), pj = (int)(q % g.nx_dom);
     const long long o = (long long)(pi + g.z0) * g.P + pj + g.pad;
-    float *dst = snap + (long long)s * slots * 3 * g.nd + q;
+    float *dst = snap + (long long)s * slots * g.snf * g.nd + q;
 #pragma unroll
     for (int f = 0; f < 3; ++f) dst[f * g.nd] = F[((long long)s * F_N + F_EX + f) * g.fstride + o];
+    if (g.snf == 5) {
+        dst[3 * g.nd] = F[((long long)s * F_N + F_U) * g.fstride + o];
+        dst[4 * g.nd] = F[((long long)s * F_N + F_V) * g.fstride + o];
+    }
 }
 
 void snap_state(stfwi_handle *h, cudaStream_t st)
@@ -745,8 +758,8 @@ stfwi_status setup_tma_kernels(stfwi_handle *h)
     }
     const void *const kern[7] = {
         (const void *)k4_fwd_vel<FD>, (const void *)k4_fwd_str<FD, false>, (const void *)k4_adj_a<FD>,
-        (const void *)k4_adj_b<FD, true, false>, (const void *)k4_adj_b<FD, true, true>,
-        (const void *)k4_adj_b<FD, false, true>, (const void *)k4_adj_b<FD, false, false>};
+        (const void *)k4_adj_b<FD, true, false, false>, (const void *)k4_adj_b<FD, true, true, false>,
+        (const void *)k4_adj_b<FD, false, true, false>, (const void *)k4_adj_b<FD, false, false, false>};
     stfwi_status r = set_smem<L4<FD>>(h, kern);
     if (r) return r;
     CK(h, cudaFuncSetAttribute((const void *)k4_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -807,6 +820,9 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     if (!d || !out) return STFWI_ERR_INVALID;
     *out = nullptr;
     if (d->fd_order != 2 && d->fd_order != 4 && d->fd_order != 8) return STFWI_ERR_UNSUPPORTED;
+    // the velocity history of the density gradient is written by the default kernels only
+    if (d->want_gradient == 2 && d->kernel_variant != 0) return STFWI_ERR_UNSUPPORTED;
+    if (d->want_gradient < 0 || d->want_gradient > 2) return STFWI_ERR_INVALID;
     const int H = d->fd_order / 2;
     if (d->nz_dom < 1 || d->nx_dom < 1 || d->pad < H || d->nt < 1 || d->nrec < 0 || d->max_shots < 1 ||
         !(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0))
@@ -855,6 +871,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.inv2dx = (float)(1.0 / (2.0 * d->dx)); g.inv2dz = (float)(1.0 / (2.0 * d->dz));
     g.dtdxdz = (float)(d->dt / (d->dx * d->dz));
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
+    g.snf = d->want_gradient == 2 ? 5 : 3;
+    h->accp = g.snf == 5 ? 7 : 5;
     h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
     h->spg = (d->max_shots + h->groups - 1) / h->groups;
     h->variant = (d->kernel_variant == 1 || d->kernel_variant == 2) ? d->kernel_variant : 0;
@@ -881,7 +899,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         h->acc_groups = h->groups;
     }
     h->acc_used = h->acc_groups;
-    h->slots = k + 1;
+    h->slots = k + 1 + ((g.snf == 5 && h->ncp > 0) ? 1 : 0);
 
     auto alloc = [&](void **ptr, size_t bytes) -> bool {
         if (bytes == 0) { *ptr = nullptr; return true; }
@@ -919,7 +937,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
               alloc((void **)&h->CKPX, (size_t)h->ncp * S * PX_NFWD * p.nz * p.xs_n * 4) &&
               alloc((void **)&h->CKPZ, (size_t)h->ncp * S * PZ_NFWD * p.zs_n * p.P * 4);
     }
-    ok &= alloc((void **)&h->acc, (size_t)h->acc_groups * 5 * nd * 8) &&
+    ok &= alloc((void **)&h->acc, (size_t)h->acc_groups * h->accp * nd * 8) &&
           alloc((void **)&h->accLr, (size_t)std::max(h->acc_groups, d->max_shots) * std::max(d->nx_dom, 1) * 8) &&
           alloc((void **)&h->gtmp, (size_t)6 * nd * 8);
     ok &= alloc((void **)&h->energy, (size_t)p.nz * p.nx * 8);
@@ -1201,13 +1219,17 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
         const int thr = 256;
         if (g.nrec > 0)
             k_inject_last<<<(g.nshot * g.nrec + thr - 1) / thr, thr, 0, s>>>(g, h->rx, h->rz, h->rec_adj, h->A);
-        auto adj = [&](int n, int seg0) {
+        auto adj = [&](int n, int seg0, int seg1) {
             const int ping = (g.nt - 1 - n) & 1;
             AdjIn ai{};
             ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = n - seg0;
             ai.accLr = h->accLr; ai.want_exact = ex; ai.ping = ping;
             AdjOut ao{};
             ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = n - seg0; ao.slot_img = n - seg0 + 1;
+            ao.accp = h->accp;
+            // outputs of step n + 1: the next slot inside a segment, else the
+            // extra slot filled from the following segment (checkpoints)
+            ao.slot_next = (n + 1 < seg1) ? n - seg0 + 2 : (h->ncp > 0 && n + 1 < g.nt ? h->ck + 1 : -1);
             ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im;
             ao.src_a = sr ? src_dev : nullptr; ao.rec_adj = h->rec_adj; ao.ping = ping;
             switch (h->d.fd_order) {
@@ -1221,6 +1243,14 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
             // segment's history, run its adjoint steps
             for (int c = h->ncp - 1; c >= 0; --c) {
                 const int seg0 = c * h->ck, seg1 = std::min(seg0 + h->ck, g.nt);
+                if (g.snf == 5 && c + 1 < h->ncp) {
+                    // keep the velocities of step seg1 (slot 1 of the segment
+                    // just processed) for the density term of step seg1 - 1
+                    const size_t ps = (size_t)h->slots * g.snf * g.nd * sizeof(float);
+                    CK(h, cudaMemcpy2DAsync(h->snap + ((size_t)h->ck + 1) * g.snf * g.nd + 3 * g.nd, ps,
+                                            h->snap + (size_t)g.snf * g.nd + 3 * g.nd, ps,
+                                            (size_t)2 * g.nd * sizeof(float), h->nshot, cudaMemcpyDeviceToDevice, s));
+                }
                 r = copy_ckpt(h, c, false, s);
                 if (r) return r;
                 snap_state(h, s);
@@ -1232,13 +1262,13 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
                     o.slot_row0 = n - seg0;
                     fwd_step(h, n, o, s);
                 }
-                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0);
+                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0, seg1);
             }
         } else {
-            for (int n = g.nt - 1; n >= 0; --n) adj(n, 0);
+            for (int n = g.nt - 1; n >= 0; --n) adj(n, 0, g.nt);
         }
         if (ex || im)
-            k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->acc_used, h->lr_used, h->acc, h->accLr, h->L2M,
+            k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->acc_used, h->accp, h->lr_used, h->acc, h->accLr, h->L2M,
                                                                       h->L, h->vs, h->vp, h->rho, ex, im,
                                                                       h->gtmp, h->gtmp + 3 * g.nd);
         CK(h, cudaGetLastError());

@@ -40,23 +40,42 @@ def _stream():
     return None
 
 
+def _want_gradient(want_gradient, density):
+    """stfwi_desc.want_gradient: 0 none, 1 stress history, 2 stress and
+    velocity history (the density gradient g_rho needs the velocities)."""
+    if not want_gradient:
+        return 0
+    return 2 if density else 1
+
+
 class Solver:
     """Batch of shots on one model; mirrors the arguments of the reference's
-    forward_jax / build_forward_fn (fwi/forward.py:119-123, :508-509)."""
+    forward_jax / build_forward_fn (fwi/forward.py:119-123, :508-509).
+
+    ``density=True`` keeps the forward velocities in the gradient history so
+    that ``gradient()`` also returns g_rho (the reference's invert='all'):
+    dJ/drho of the exact gradient, and the imaging formula's density term."""
 
     def __init__(self, nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, max_shots, fd_order=2,
                  free_surface=True, want_gradient=True, shot_group=0, mem_budget_gb=0.0,
-                 kernel_variant=0, ckpt_interval=0):
+                 kernel_variant=0, ckpt_interval=0, density=False):
         if fd_order not in (2, 4, 8):
             raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
         self.lib = N.load()
+        self.density = bool(density and want_gradient)
         self.desc = N.StfwiDesc(int(nz_dom), int(nx_dom), int(pad), int(fd_order),
                                 int(bool(free_surface)), int(nt), int(nrec), int(max_shots),
-                                float(dx), float(dz), float(dt), float(fc), int(bool(want_gradient)),
+                                float(dx), float(dz), float(dt), float(fc),
+                                _want_gradient(want_gradient, density),
                                 int(shot_group), float(mem_budget_gb), int(kernel_variant),
                                 int(ckpt_interval))
         h = ct.c_void_p()
         st = self.lib.stfwi_create(ct.byref(self.desc), ct.byref(h))
+        if st == N.STFWI_ERR_UNSUPPORTED:
+            raise NotImplementedError(f"stfwi_create: unsupported configuration {self.shape_desc()}"
+                                      + (" (the density gradient needs kernel_variant 0)" if density else ""))
+        if st == N.STFWI_ERR_INVALID:
+            raise ValueError(f"stfwi_create: invalid descriptor {self.shape_desc()}")
         if st != N.STFWI_OK:
             raise N.StfwiError(st, f"stfwi_create failed for {self.shape_desc()}")
         self.h = h
@@ -77,7 +96,8 @@ class Solver:
         lib = N.load()
         d = N.StfwiDesc(kw["nz_dom"], kw["nx_dom"], kw["pad"], kw.get("fd_order", 2),
                         int(kw.get("free_surface", True)), kw["nt"], kw["nrec"], kw["max_shots"],
-                        kw["dx"], kw["dz"], kw["dt"], kw["fc"], int(kw.get("want_gradient", True)),
+                        kw["dx"], kw["dz"], kw["dt"], kw["fc"],
+                        _want_gradient(kw.get("want_gradient", True), kw.get("density", False)),
                         kw.get("shot_group", 0), kw.get("mem_budget_gb", 0.0),
                         kw.get("kernel_variant", 0), kw.get("ckpt_interval", 0))
         return int(lib.stfwi_workspace_bytes(ct.byref(d)))
@@ -185,6 +205,8 @@ class Solver:
     def gradient(self, exact=True, imaging=False, src=False, out=None, sync=True):
         """Adjoint sweep.  Returns a dict with 'exact' / 'imaging' ->
         (g_Vs, g_Vp, g_rho) FP64 arrays and 'src' -> [nshot, nt] float32.
+        The exact g_rho is zero unless the solver was made with density=True;
+        the imaging g_rho then includes the density (velocity) term.
         ``out`` may be a device tensor [n_modes, 3, nz_dom, nx_dom] float64."""
         mode = (N.GRAD_EXACT if exact else 0) | (N.GRAD_IMAGING if imaging else 0) | (N.GRAD_SRC if src else 0)
         nmat = int(exact) + int(imaging)

@@ -54,6 +54,24 @@ def test_create_rejects_bad_descriptors_before_touching_a_device():
     assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
     d.pad, d.dt = 8, -1.0
     assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
+    d.dt = 1e-3
+    d.want_gradient, d.kernel_variant = 2, 1   # the velocity history exists in variant 0 only
+    assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_UNSUPPORTED
+    d.want_gradient, d.kernel_variant = 3, 0
+    assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
+
+
+def test_density_history_holds_five_fields_per_step():
+    """want_gradient = 2 (density gradient) keeps U and V beside the three
+    stresses: 5/3 of the history bytes, plus one extra slot with checkpoints."""
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    d = N.StfwiDesc(152, 500, 20, 8, 1, 2000, 250, 50, 20.0, 20.0, 1.5e-3, 5.0, 1, 0, 0.0, 0, 0)
+    w1 = lib.stfwi_workspace_bytes(ct.byref(d))
+    d.want_gradient = 2
+    w2 = lib.stfwi_workspace_bytes(ct.byref(d))
+    hist = 50 * 2001 * 3 * 152 * 500 * 4
+    assert abs((w2 - w1) - 2 * hist / 3) < 0.01 * hist, (w1, w2)
 
 
 def test_noalloc_size_check_runs_on_the_host():

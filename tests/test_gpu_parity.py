@@ -259,3 +259,84 @@ def test_multi_tile_grid_vs_oracle(fd, fs, variant):
     tol = 2e-5 * max(amp, 1.0)
     assert all(e < tol for e in errs.values()), (tol, errs)
     S.close()
+
+
+def _density_case(fd, fs, st, big, nt):
+    if big:
+        nz, nx, pad, dx, dt, fc = 70, 150, 10, 10.0, 1.0e-3, 18.0
+        vs, vp, rho = _smooth_model(nz, nx, 11)
+        rx = np.arange(0, nx, 3, dtype=np.int32)
+        rz = np.full_like(rx, 0 if fs else 3)
+        sx, sz = np.array([54, 70]), np.array([22, 47])
+        types = [st, "force"]
+    else:
+        nz, nx, pad, dx, dt, fc = C.NZ, C.NX, C.PAD, C.DX, C.DT, C.FC
+        vs, vp, rho = C.model()
+        sx0, sz0, rx, rz = C.acquisition(fs, st)
+        sx, sz, types = np.array([sx0]), np.array([sz0]), [st]
+    wav = O.ricker(np.arange(nt) * dt, fc, 1.5 / fc) * 1e9
+    geo = dict(rec_x=rx, rec_z=rz, nx_dom=nx, nz_dom=nz, dx=dx, dz=dx, dt=dt, nt=nt, fc=fc, pad=pad,
+               fd_order=fd, free_surface=fs, d0_f32=True)
+    obs = O.forward_batch(vs * 1.02, vp, rho * 1.01, sx, sz, types, src_wavelet=wav, **geo)[:, 1]
+    return vs, vp, rho, sx, sz, types, wav, geo, obs
+
+
+@pytest.mark.parametrize("fd,fs,st,big", [(8, True, "force", False), (8, True, "moment", False),
+                                          (4, False, "force", False), (8, True, "moment", True)])
+def test_density_gradient_vs_oracle(fd, fs, st, big):
+    """invert='all': the exact g_rho (buoyancy, moment and free-surface terms
+    through rho) and the imaging g_rho with its velocity term
+    (fwi/imaging.py:145-154) against the FP64 oracle; g_Vs and g_Vp are the
+    same with and without the velocity history."""
+    nt = 110
+    vs, vp, rho, sx, sz, types, wav, geo, obs = _density_case(fd, fs, st, big, nt)
+    kw = dict(src_x=sx, src_z=sz, src_wavelet=wav, observed=obs, src_types=types, component=1,
+              scale=1.0, invert="all", **geo)
+    (gx_vs, gx_vp, gx_rho), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
+    (gi_vs, gi_vp, gi_rho), _ = O.compute_gradient("adjoint", Vs=vs, Vp=vp, rho=rho, **kw)
+    g = {}
+    for density in (False, True):
+        S = _solver(nt, len(geo["rec_x"]), len(sx), fd, geo["free_surface"], want_gradient=True,
+                    pad=geo["pad"], nz=geo["nz_dom"], nx=geo["nx_dom"], dx=geo["dx"], dz=geo["dz"],
+                    dt=geo["dt"], fc=geo["fc"], density=density)
+        S.set_model(vs, vp, rho)
+        S.set_receivers(geo["rec_x"], geo["rec_z"])
+        S.set_shots(sx, sz, types, wav.astype(np.float32))
+        S.forward(store=True)
+        mis = S.misfit(obs.astype(np.float32), 1, 1.0)
+        rec = S.records()[:, 1].astype(np.float64)
+        amp = float(np.linalg.norm(rec) / np.linalg.norm(rec - obs))
+        g[density] = S.gradient(exact=True, imaging=True)
+        S.close()
+    for k in ("exact", "imaging"):
+        for c in (0, 1):
+            assert _rel(g[True][k][c], g[False][k][c]) < 1e-12, (k, c)
+    assert np.all(g[False]["exact"][2] == 0.0)
+    errs = {"misfit": abs(mis.sum() / loss - 1), "exact_rho": _rel(g[True]["exact"][2], gx_rho),
+            "img_rho": _rel(g[True]["imaging"][2], gi_rho), "exact_vs": _rel(g[True]["exact"][0], gx_vs)}
+    print(f"density fd{fd} fs={fs} {st} big={big}: amplification {amp:.1f} errors {errs}")
+    tol = 2e-5 * max(amp, 1.0)
+    assert all(e < tol for e in errs.values()), (tol, errs)
+
+
+def test_density_gradient_checkpointed_equals_store_all():
+    """With the velocity history, checkpoint segments (k = 7, not dividing
+    nt) give the every-step result: the imaging density term of a segment's
+    last step reads the first output of the following segment."""
+    nt = 100
+    vs, vp, rho, sx, sz, types, wav, geo, obs = _density_case(8, True, "moment", True, nt)
+    out = []
+    for ck in (0, 7):
+        S = _solver(nt, len(geo["rec_x"]), len(sx), 8, True, want_gradient=True, pad=geo["pad"],
+                    nz=geo["nz_dom"], nx=geo["nx_dom"], dx=geo["dx"], dz=geo["dz"], dt=geo["dt"],
+                    fc=geo["fc"], density=True, ckpt_interval=ck)
+        S.set_model(vs, vp, rho)
+        S.set_receivers(geo["rec_x"], geo["rec_z"])
+        S.set_shots(sx, sz, types, wav.astype(np.float32))
+        S.forward(store=True)
+        S.misfit(obs.astype(np.float32), 1, 1.0)
+        g = S.gradient(exact=True, imaging=True)
+        out.append([g["exact"][2], g["imaging"][2], g["exact"][0]])
+        S.close()
+    for a, b in zip(out[1], out[0]):
+        assert _rel(a, b) < 1e-12, _rel(a, b)

@@ -123,6 +123,31 @@ def test_exact_gradient_vp_rho_finite_difference(param):
     _fd_check(param, True, "force", 4, comp=1)
 
 
+@pytest.mark.parametrize("ckpt", [7, 100])
+def test_imaging_density_term_matches_history_formula(ckpt):
+    """The density term of the imaging condition (third imaging plane) is
+    fwi/imaging.py:145-154 applied to the forward velocity history and the
+    adjoint velocity history, also when the recompute runs in checkpoint
+    segments that do not divide nt."""
+    vs, vp, rho = C.model()
+    nt, fs, st, fd = 40, True, "force", 4
+    sx, sz, rx, rz = C.acquisition(fs, st)
+    wav = O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9
+    rng = np.random.default_rng(8)
+    ys = [rng.standard_normal((nt, len(rx))) for _ in range(4)]
+    _, full, _ = O.forward(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, nt, C.FC, C.PAD,
+                           wav, fd, fs, st, full=("vx", "vz"))
+    a = O.adjoint(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, nt, C.FC, C.PAD, *ys,
+                  fd_order=fd, free_surface=fs, src_type=st, src_wavelet=wav, want=("img",),
+                  hist=("U_a", "V_a"), ckpt=ckpt)
+    vx, vz, ua, va = full["vx"], full["vz"], a["U_a"], a["V_a"]
+    ref = np.zeros_like(vx[0])
+    for n in range(1, nt - 1):
+        ref -= C.DT * (vx[n] * (ua[n + 1] - ua[n - 1]) + vz[n] * (va[n + 1] - va[n - 1])) / (2 * C.DT)
+    assert np.abs(ref).max() > 0
+    np.testing.assert_allclose(a["img"][2], ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
 @pytest.mark.slow
 def test_known_answers_gradient_compare(known_answers):
     """Results_gradient/gradient_compare.npz (compute_gradient_handcoded.py):
