@@ -173,6 +173,36 @@ stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t nrec, const
                                   const float *obs, const stfwi_misfit_desc *m, float *rec_adj,
                                   double *misfit_out, void *stream);
 
+/* Gradient post-processing applied on the device to every plane that
+ * stfwi_gradient returns (fwi/gradient.py:266-277 _postprocess): Gaussian
+ * smoothing with sigma grad_smooth_sigma (fwi/loss.py:17-30; 0 = none, at
+ * most sigma 21), then the product with source_taper and with illumination
+ * ([nz_dom][nx_dom] FP64, host or device, copied; null = none).  Stays set
+ * for the following stfwi_gradient calls. */
+stfwi_status stfwi_set_postprocess(stfwi_handle *h, double grad_smooth_sigma, const double *source_taper,
+                                   const double *illumination, void *stream);
+
+enum { STFWI_PRECOND_ILLUM = 0, STFWI_PRECOND_EPRECOND3 = 1 };
+
+/* Gradient preconditioner from the forward energy Ws = sum_shots sum_t
+ * field(component)^2 of the handle's model and shots, computed on the
+ * device, written to out [nz_dom][nx_dom] FP64 (host or device), normalised
+ * to max 1.  STFWI_PRECOND_ILLUM: 1 / (Ws + eps max Ws) on the physical grid
+ * (fwi/illumination.py:18-48 compute_illumination_for_stage; the reference's
+ * forward there injects forces, so set force shots to reproduce it).
+ * STFWI_PRECOND_EPRECOND3: 1 / We with We the Plessix-Mulder energy of the
+ * receiver line (fwi/preconditioning.py:65-139 eprecond3, as used by
+ * fwi/optim_lbfgsb.py:51-100). */
+stfwi_status stfwi_preconditioner(stfwi_handle *h, int32_t kind, int32_t component, double eps, double *out,
+                                  void *stream);
+
+/* Velocity feasibility projection in place on device FP64 arrays of n cells
+ * (fwi/projections.py:67-117 project_velocity): Vp <= vp_cap (vp_cap <= 0:
+ * no cap), Vs <= Vp / ((1 + K_margin) 2/sqrt(3)), Vs >= vs_floor, rho >=
+ * rho_floor.  No handle; host pointers return STFWI_ERR_INVALID. */
+stfwi_status stfwi_project_velocity(int64_t n, double *vs, double *vp, double *rho, double K_margin, double vp_cap,
+                                    double vs_floor, double rho_floor, void *stream);
+
 /* Padded-grid shape of a descriptor. */
 void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t);
 

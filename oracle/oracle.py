@@ -447,3 +447,46 @@ def compute_illumination(nz, nx, dx, dz, dt, nt, f_c, pad, rec_x, rec_z, fd_orde
     lamda = eps * np.max(Ws)
     H_inv = 1.0 / (Ws + lamda)
     return H_inv / np.max(H_inv), Ws
+
+
+# ---------------------------------------------------------------- host pieces around the gradient
+
+def project_velocity(Vs, Vp, rho, K_margin=0.04, vp_cap=None, vs_floor=1e-3, rho_floor=1e-3):
+    """fwi/projections.py:67-117: Vp <= vp_cap, Vs <= Vp / ((1 + K) 2/sqrt 3),
+    floors on Vs and rho (FP64 copies)."""
+    vp = np.asarray(Vp, dtype=np.float64).copy()
+    vs = np.asarray(Vs, dtype=np.float64).copy()
+    rh = np.asarray(rho, dtype=np.float64).copy()
+    r = (1.0 + float(K_margin)) * (2.0 / np.sqrt(3.0))
+    if vp_cap is not None:
+        vp = np.minimum(vp, float(vp_cap))
+    vs = np.maximum(np.minimum(vs, vp / r), float(vs_floor))
+    rh = np.maximum(rh, float(rho_floor))
+    return vs, vp, rh
+
+
+def illumination_inverse(Ws_padded, nz_dom, nx_dom, pad, eps):
+    """fwi/illumination.py:44-47 on a forward energy of the padded grid
+    (free surface: rows from 0)."""
+    Ws = np.asarray(Ws_padded)[:nz_dom, pad:pad + nx_dom]
+    h = 1.0 / (Ws + eps * np.max(Ws))
+    return h / np.max(h)
+
+
+def eprecond3_multiplier(Ws_padded, rec_x, rec_z, dx, dz, free_surface, pad, nz_dom, nx_dom, eps):
+    """fwi/preconditioning.py:65-139 (We on the padded grid) followed by
+    fwi/optim_lbfgsb.py:95-99 (crop, 1/We, normalised to max 1)."""
+    Ws = np.asarray(Ws_padded, dtype=np.float64)
+    nz_t, nx_t = Ws.shape
+    z0 = 0 if free_surface else pad
+    cz, cx = np.meshgrid((np.arange(nz_t) - z0) * dz, (np.arange(nx_t) - pad) * dx, indexing="ij")
+    rec_x, rec_z = np.asarray(rec_x), np.asarray(rec_z)
+    if np.std(rec_x) >= np.std(rec_z):
+        lo, hi, perp, c_perp, c_line, sp = np.min(rec_x) * dx, np.max(rec_x) * dx, rec_z[0] * dz, cz, cx, dz
+    else:
+        lo, hi, perp, c_perp, c_line, sp = np.min(rec_z) * dz, np.max(rec_z) * dz, rec_x[0] * dx, cx, cz, dx
+    y = np.maximum(np.abs(c_perp - perp), sp)
+    We = np.abs(np.sqrt(Ws) * (np.arcsinh((hi - c_line) / y) - np.arcsinh((lo - c_line) / y)))
+    We = We + eps * np.max(We)
+    p = 1.0 / We[z0:z0 + nz_dom, pad:pad + nx_dom]
+    return p / np.max(p)

@@ -962,7 +962,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
         const float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
         const float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
-        const float *snap_in = (EXACT && o.slot_in >= 0)
+        const float *snap_in = ((EXACT || (IMG && RHO)) && o.slot_in >= 0)
                                    ? o.snap + ((long long)s * o.slots + o.slot_in) * g.snf * g.nd : nullptr;
         const float *snap_img = ((IMG || RHO) && o.slot_img >= 0)
                                     ? o.snap + ((long long)s * o.slots + o.slot_img) * g.snf * g.nd : nullptr;

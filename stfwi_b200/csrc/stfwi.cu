@@ -19,6 +19,7 @@
 #include "kernels.cuh"
 #include "kernels_v3.cuh"
 #include "kernels_v4.cuh"
+#include "post.cuh"
 
 using namespace stfwi;
 
@@ -77,6 +78,16 @@ struct stfwi_handle {
     float *wav = nullptr, *fcoef = nullptr, *mcoef = nullptr, *lm = nullptr;
     int *tile_start = nullptr, *tile_rec = nullptr, *rx = nullptr, *rz = nullptr;
     bool shots_set = false, recv_set = false;
+    std::vector<int> rec_x_h, rec_z_h;   // physical-domain receiver indices (preconditioner geometry)
+
+    // gradient post-processing (fwi/gradient.py:266-277) and preconditioners
+    double post_sigma = 0.0;
+    int post_radius = 0;
+    bool post_taper = false, post_illum = false;
+    double *pw = nullptr;      // Gaussian weights [2 * POST_MAX_RADIUS + 1]
+    double *ptaper = nullptr, *pillum = nullptr, *ptmp = nullptr;   // [nd] each
+    double *pscr = nullptr;    // [nz][nx] scratch (eprecond3)
+    double *pmax = nullptr;    // reductions
 
     // state
     float *F = nullptr, *A = nullptr, *PX = nullptr, *PZ = nullptr;
@@ -174,7 +185,8 @@ Plan make_plan(const stfwi_desc *d, int k)
     p.acc = (size_t)G * ((snf == 5 ? 7 : 5) * p.nd + d->nx_dom) * sizeof(double) + 3 * p.nd * 2 * sizeof(double);
     p.rec = (size_t)2 * S * 4 * d->nt * std::max(d->nrec, 1) * sizeof(float)
           + (size_t)S * d->nt * std::max(d->nrec, 1) * sizeof(float);
-    p.misc = (size_t)(8 * p.nz * p.P + 4 * p.nd) * sizeof(float) + (size_t)p.nz * p.nx * sizeof(double)
+    p.misc = (size_t)(8 * p.nz * p.P + 4 * p.nd) * sizeof(float) + (size_t)2 * p.nz * p.nx * sizeof(double)
+           + (size_t)3 * p.nd * sizeof(double)
            + (size_t)S * (d->nt + 16) * sizeof(float) + (size_t)S * (std::max(d->nrec, 1) + 1) * sizeof(double)
            + (1 << 20);
     return p;
@@ -941,6 +953,9 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
           alloc((void **)&h->accLr, (size_t)std::max(h->acc_groups, d->max_shots) * std::max(d->nx_dom, 1) * 8) &&
           alloc((void **)&h->gtmp, (size_t)6 * nd * 8);
     ok &= alloc((void **)&h->energy, (size_t)p.nz * p.nx * 8);
+    ok &= alloc((void **)&h->pw, (2 * POST_MAX_RADIUS + 1) * 8) && alloc((void **)&h->ptaper, (size_t)nd * 8) &&
+          alloc((void **)&h->pillum, (size_t)nd * 8) && alloc((void **)&h->ptmp, (size_t)nd * 8) &&
+          alloc((void **)&h->pscr, (size_t)p.nz * p.nx * 8) && alloc((void **)&h->pmax, 64);
     ok &= alloc((void **)&h->mis_trace, (size_t)S * nrec * 8) && alloc((void **)&h->mis_shot, (size_t)S * 8);
     ok &= alloc((void **)&h->src_a, (size_t)S * d->nt * 4);
     if (!ok) {
@@ -980,7 +995,8 @@ void stfwi_destroy(stfwi_handle *h)
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
                     h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
-                    h->mis_trace, h->mis_shot, h->src_a, h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->CKF, h->CKPX,
+                    h->mis_trace, h->mis_shot, h->src_a, h->pw, h->ptaper, h->pillum, h->ptmp, h->pscr, h->pmax,
+                    h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->CKF, h->CKPX,
                     h->CKPZ};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -1059,6 +1075,8 @@ stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *r
     stfwi_status gr;
     if ((gr = group(h->tha, h->ntza, h->tile_startA, h->tile_recA))) return gr;
     if ((gr = group(h->thb, h->ntzb, h->tile_startB, h->tile_recB))) return gr;
+    h->rec_x_h.assign(rec_x, rec_x + nrec);
+    h->rec_z_h.assign(rec_z, rec_z + nrec);
     h->recv_set = true;
     return STFWI_OK;
 }
@@ -1280,6 +1298,23 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
         prof_accumulate(h, 2);
         prof_accumulate(h, 3);
     }
+    if ((ex || im) && (h->post_radius > 0 || h->post_taper || h->post_illum)) {
+        // fwi/gradient.py:266-277 on the device: Gaussian smoothing, then the
+        // source taper and the illumination multiplies, on every output plane
+        double *base = ex ? h->gtmp : h->gtmp + 3 * g.nd;
+        const int planes = 3 * (int(ex) + int(im));
+        const unsigned nb = (unsigned)((g.nd + 255) / 256);
+        if (h->post_radius > 0)
+            for (int p = 0; p < planes; ++p) {
+                double *pl = base + (size_t)p * g.nd;
+                k_gauss_axis<<<nb, 256, 0, st>>>(g.nz_dom, g.nx_dom, 1, h->post_radius, h->pw, pl, h->ptmp);
+                k_gauss_axis<<<nb, 256, 0, st>>>(g.nz_dom, g.nx_dom, 0, h->post_radius, h->pw, h->ptmp, pl);
+            }
+        if (h->post_taper || h->post_illum)
+            k_mul_planes<<<nb, 256, 0, st>>>(g.nd, planes, base, h->post_taper ? h->ptaper : nullptr,
+                                             h->post_illum ? h->pillum : nullptr);
+        CK(h, cudaGetLastError());
+    }
     if (sr) CK(h, cudaMemcpyAsync(src_wav_a, src_dev, (size_t)h->nshot * g.nt * 4, cudaMemcpyDefault, st));
     size_t off = 0;
     if (ex) {
@@ -1302,6 +1337,125 @@ stfwi_status stfwi_illumination(stfwi_handle *h, int32_t component, double *ws_o
     h->stored = false;
     CK(h, cudaMemcpyAsync(ws_out, h->energy, (size_t)h->g.nz * h->g.nx * 8, cudaMemcpyDefault,
                           (cudaStream_t)stream));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_postprocess(stfwi_handle *h, double grad_smooth_sigma, const double *source_taper,
+                                   const double *illumination, void *stream)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    if (!(grad_smooth_sigma >= 0.0)) return fail(h, STFWI_ERR_INVALID, "grad_smooth_sigma must be >= 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    int radius = 0;
+    if (grad_smooth_sigma > 0.0) {
+        // fwi/loss.py:17-30: truncate = 3, radius = int(3 sigma + 0.5), normalised weights
+        radius = (int)(3.0 * grad_smooth_sigma + 0.5);
+        if (radius > POST_MAX_RADIUS)
+            return fail(h, STFWI_ERR_INVALID, "grad_smooth_sigma %g needs a radius above %d", grad_smooth_sigma,
+                        POST_MAX_RADIUS);
+        std::vector<double> w(2 * radius + 1);
+        double sum = 0.0;
+        for (int k = -radius; k <= radius; ++k) {
+            const double x = k / grad_smooth_sigma;
+            w[k + radius] = std::exp(-0.5 * x * x);
+            sum += w[k + radius];
+        }
+        for (double &v : w) v /= sum;
+        CK(h, cudaMemcpyAsync(h->pw, w.data(), w.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(h, cudaStreamSynchronize(st));
+    }
+    if (source_taper) CK(h, cudaMemcpyAsync(h->ptaper, source_taper, (size_t)g.nd * 8, cudaMemcpyDefault, st));
+    if (illumination) CK(h, cudaMemcpyAsync(h->pillum, illumination, (size_t)g.nd * 8, cudaMemcpyDefault, st));
+    CK(h, cudaStreamSynchronize(st));
+    h->post_sigma = grad_smooth_sigma;
+    h->post_radius = radius;
+    h->post_taper = source_taper != nullptr;
+    h->post_illum = illumination != nullptr;
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_preconditioner(stfwi_handle *h, int32_t kind, int32_t component, double eps, double *out,
+                                  void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if ((kind != STFWI_PRECOND_ILLUM && kind != STFWI_PRECOND_EPRECOND3) || component < 0 || component > 3 || !out ||
+        !(eps >= 0.0))
+        return fail(h, STFWI_ERR_INVALID, "bad preconditioner request");
+    if (kind == STFWI_PRECOND_EPRECOND3 && h->rec_x_h.empty())
+        return fail(h, STFWI_ERR_STATE, "eprecond3 needs receivers");
+    cudaStream_t st = (cudaStream_t)stream;
+    GraphKey key{2, (uint32_t)component, h->nshot};
+    rc = run_graph(h, key, st, [&](cudaStream_t s) { return enqueue_forward(h, 0, component, s); });
+    if (rc) return rc;
+    h->stored = false;
+    const Geo &g = h->g;
+    const long long n = g.nd, np = (long long)g.nz * g.nx;
+    const unsigned nb = (unsigned)((n + 255) / 256), npb = (unsigned)((np + 255) / 256);
+    double *res;
+    if (kind == STFWI_PRECOND_ILLUM) {
+        // fwi/illumination.py:44-47: crop, H = 1/(Ws + eps max Ws), H / max H
+        k_crop<<<nb, 256, 0, st>>>(g.nz_dom, g.nx_dom, g.nx, g.z0, g.pad, h->energy, h->ptmp);
+        k_max_1block<<<1, 1024, 0, st>>>(n, h->ptmp, h->pmax);
+        k_illum_inverse<<<nb, 256, 0, st>>>(n, h->ptmp, h->pmax, eps, h->pscr);
+        res = h->pscr;
+    } else {
+        // fwi/preconditioning.py:65-139 + fwi/optim_lbfgsb.py:95-99: the
+        // receiver line's orientation is the coordinate with the larger spread
+        auto stdev = [](const std::vector<int> &v) {
+            double m = 0, q = 0;
+            for (int x : v) m += x;
+            m /= (double)v.size();
+            for (int x : v) q += (x - m) * (x - m);
+            return std::sqrt(q / (double)v.size());
+        };
+        const auto &rx = h->rec_x_h, &rz = h->rec_z_h;
+        const bool horiz = stdev(rx) >= stdev(rz);
+        const double dx = h->d.dx, dz = h->d.dz;
+        const double lmin = horiz ? *std::min_element(rx.begin(), rx.end()) * dx : *std::min_element(rz.begin(), rz.end()) * dz;
+        const double lmax = horiz ? *std::max_element(rx.begin(), rx.end()) * dx : *std::max_element(rz.begin(), rz.end()) * dz;
+        const double perp = horiz ? rz[0] * dz : rx[0] * dx;
+        k_eprecond3_we<<<npb, 256, 0, st>>>(g.nz, g.nx, g.z0, g.pad, dx, dz, horiz ? 1 : 0, lmin, lmax, perp, h->energy,
+                                            h->pscr);
+        k_max_1block<<<1, 1024, 0, st>>>(np, h->pscr, h->pmax);
+        k_eprecond3_inv<<<nb, 256, 0, st>>>(g.nz_dom, g.nx_dom, g.nx, g.z0, g.pad, h->pscr, h->pmax, eps, h->ptmp);
+        res = h->ptmp;
+    }
+    k_max_1block<<<1, 1024, 0, st>>>(n, res, h->pmax + 1);
+    k_scale_by_inverse_max<<<nb, 256, 0, st>>>(n, res, h->pmax + 1);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(out, res, (size_t)n * 8, cudaMemcpyDefault, st));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_project_velocity(int64_t n, double *vs, double *vp, double *rho, double K_margin, double vp_cap,
+                                    double vs_floor, double rho_floor, void *stream)
+{
+    if (n < 0 || !vs || !vp || !rho || !(K_margin > -1.0)) {
+        fprintf(stderr, "stfwi_project_velocity: invalid arguments\n");
+        return STFWI_ERR_INVALID;
+    }
+    if (n == 0) return STFWI_OK;
+    for (const double *ptr : {(const double *)vs, (const double *)vp, (const double *)rho}) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess ||
+            (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)) {
+            cudaGetLastError();
+            fprintf(stderr, "stfwi_project_velocity: the model arrays must be device memory\n");
+            return STFWI_ERR_INVALID;
+        }
+    }
+    // fwi/projections.py:37-48: r = (1 + K_margin) * 2/sqrt(3)
+    const double r = (1.0 + K_margin) * (2.0 / std::sqrt(3.0));
+    const int use_cap = (vp_cap > 0.0 && std::isfinite(vp_cap)) ? 1 : 0;
+    k_project_velocity<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n, vs, vp, rho, r, vp_cap,
+                                                                                   use_cap, vs_floor, rho_floor);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "stfwi_project_velocity: %s\n", cudaGetErrorString(e));
+        return STFWI_ERR_CUDA;
+    }
     return STFWI_OK;
 }
 

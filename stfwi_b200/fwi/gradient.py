@@ -4,9 +4,8 @@ Backends: ``'cuda'`` (alias ``'ad'``) returns the exact gradient of the
 discrete forward, what the reference's ``'ad'`` backend gets from JAX AD;
 ``'cuda_imaging'`` (alias ``'adjoint'``) returns the reference's imaging
 condition (fwi/imaging.py), fused into the adjoint sweep.  The forward, the
-residual preparation (filter, taper, FP64 misfit) and the adjoint all run on
-the GPU; the post-processing (smoothing, source taper, illumination) is the
-reference's host arithmetic.  Unlike the reference's ``'adjoint'`` backend,
+residual preparation (filter, taper, FP64 misfit), the adjoint and the
+post-processing (smoothing, source taper, illumination) all run on the GPU.  Unlike the reference's ``'adjoint'`` backend,
 whose forward always injects a force (fwi/gradient.py:176-180), the forward
 and the adjoint here use the same ``src_type``.
 """
@@ -28,21 +27,22 @@ def clear_cache():
     _CACHE.clear()
 
 
-def _solver(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order, free_surface):
+def _solver(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order, free_surface, density=False):
     key = (nz_dom, nx_dom, float(dx), float(dz), float(dt), nt, float(fc), pad, nrec, nshot, fd_order,
-           bool(free_surface))
+           bool(free_surface), bool(density))
     S = _CACHE.get(key)
     if S is None:
         if len(_CACHE) >= 4:
             clear_cache()
         S = Solver(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, nrec, nshot, fd_order=fd_order,
-                   free_surface=free_surface, want_gradient=True)
+                   free_surface=free_surface, want_gradient=True, density=density)
         _CACHE[key] = S
     return S
 
 
 def _postprocess(grads, grad_smooth_sigma, source_taper, illumination):
-    """fwi/gradient.py:266-277."""
+    """fwi/gradient.py:266-277 on the host (build_loss_fn, whose Tikhonov
+    term is added to the gradient before this step)."""
     out = list(grads)
     if grad_smooth_sigma is not None:
         out = [gaussian_smooth_2d(g, grad_smooth_sigma) for g in out]
@@ -68,8 +68,6 @@ def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observe
         raise ValueError(f"unknown backend {backend!r}; use 'cuda' or 'cuda_imaging'")
     if invert not in ("vs", "vs_vp", "all"):
         raise ValueError(f"invert={invert!r}; use 'vs', 'vs_vp', or 'all'")
-    if invert == "all":
-        raise NotImplementedError("invert='all': the density gradient is not accumulated on the GPU")
     if fd_order not in (2, 4, 8):
         raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
     mode = _BACKENDS[backend]
@@ -81,16 +79,21 @@ def compute_gradient(backend, *, Vs, Vp, rho, src_x, src_z, src_wavelet, observe
             raise NotImplementedError(f"src_type={t!r} not supported (use 'force' or 'moment').")
     rx = np.asarray(rec_x, dtype=np.int32).reshape(-1)
     rz = np.asarray(rec_z, dtype=np.int32).reshape(-1)
+    # invert='all' keeps the forward velocities for the density gradient
     S = _solver(int(nz_dom), int(nx_dom), dx, dz, dt, int(nt), fc, int(pad), rx.size, sx.size, int(fd_order),
-                free_surface)
+                free_surface, density=(invert == "all"))
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, np.asarray(src_wavelet, dtype=np.float32))
     S.set_model(Vs, Vp, rho)
     S.forward(store=True)
     loss = float(S.misfit(observed, component, scale, sos, n_taper, nshot_norm=n_shots_total or 0).sum())
+    # fwi/gradient.py:266-277 on the device, after the adjoint sweep
+    S.set_postprocess(grad_smooth_sigma, source_taper, illumination)
     g = S.gradient(exact=(mode == "exact"), imaging=(mode == "imaging"))[mode]
     g_vs, g_vp, g_rho = (np.array(a) for a in g)
+    # fwi/gradient.py:250-257: frozen parameters get zero gradients
     if invert == "vs":
         g_vp = np.zeros_like(g_vp)
-    g_rho = np.zeros_like(g_rho)
-    return _postprocess((g_vs, g_vp, g_rho), grad_smooth_sigma, source_taper, illumination), loss
+    if invert != "all":
+        g_rho = np.zeros_like(g_rho)
+    return (g_vs, g_vp, g_rho), loss

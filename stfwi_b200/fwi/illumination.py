@@ -1,5 +1,6 @@
 """compute_illumination_for_stage with the reference's signature
-(fwi/illumination.py:18-48): Ws = Sum_shots Sum_t field^2 runs on the GPU."""
+(fwi/illumination.py:18-48): Ws = Sum_shots Sum_t field^2, the crop and the
+normalised inverse run on the GPU."""
 from __future__ import annotations
 
 import numpy as np
@@ -25,6 +26,8 @@ def compute_illumination_for_stage(nz, nx, dx, dz, dt, nt, f_c, pad, block_size,
         S.set_model(Vs, Vp, rho)
         S.set_receivers(rx, rz)
         S.set_shots(sx, sz, "force", np.asarray(src_wavelet, dtype=np.float32))
+        if not return_ws:
+            return S.preconditioner("illum", component, eps)
         Ws = S.illumination(component)
     finally:
         S.close()

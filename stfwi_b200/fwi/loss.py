@@ -38,8 +38,6 @@ def build_loss_fn(run_shot, observed, src_x_list, src_z, src_wavelet, component=
     from .gradient import _postprocess, _solver
     if invert not in ("vs", "vs_vp", "all"):
         raise ValueError(f"invert={invert!r}; use 'vs', 'vs_vp', or 'all'")
-    if invert == "all":
-        raise NotImplementedError("invert='all': the density gradient is not accumulated on the GPU")
     geo = run_shot.geo
     sx = np.asarray(src_x_list).astype(np.int64).reshape(-1)
     sz = np.full(sx.shape, int(np.asarray(src_z).reshape(-1)[0]))
@@ -48,28 +46,39 @@ def build_loss_fn(run_shot, observed, src_x_list, src_z, src_wavelet, component=
     def loss_fn(params):
         Vs, Vp, rho = params
         S = _solver(geo["nz_dom"], geo["nx_dom"], geo["dx"], geo["dz"], geo["dt"], geo["nt"], geo["fc"],
-                    geo["pad"], run_shot.rec_x.size, sx.size, geo["fd_order"], geo["free_surface"])
+                    geo["pad"], run_shot.rec_x.size, sx.size, geo["fd_order"], geo["free_surface"],
+                    density=(invert == "all"))
         S.set_receivers(run_shot.rec_x, run_shot.rec_z)
         S.set_shots(sx, sz, "force", np.asarray(src_wavelet, dtype=np.float32))
         S.set_model(Vs, Vp, rho)
         S.forward(store=True)
         total = float(S.misfit(obs, component, scale, sos, n_taper).sum())
+        S.set_postprocess(None, None, None)   # post-processing below, after the Tikhonov term
         g_vs, g_vp, g_rho = (np.array(a) for a in S.gradient(exact=True)["exact"])
+        # fwi/loss.py:73-78: frozen parameters are stop-gradient
         if invert == "vs":
             g_vp = np.zeros_like(g_vp)
-        g_rho = np.zeros_like(g_rho)
+        if invert != "all":
+            g_rho = np.zeros_like(g_rho)
         if tikhonov_alpha is not None:
+            # fwi/loss.py:91-98: first-difference penalty on the inverted
+            # parameters, weighted as a fraction of the misfit (the weight
+            # itself is stop-gradient)
             reg, dreg_vs = _diff_reg(Vs)
-            dregs = [dreg_vs, None]
-            if invert == "vs_vp":
-                r2, dreg_vp = _diff_reg(Vp)
+            dregs = [dreg_vs, None, None]
+            if invert in ("vs_vp", "all"):
+                r2, dregs[1] = _diff_reg(Vp)
                 reg += r2
-                dregs[1] = dreg_vp
+            if invert == "all":
+                r3, dregs[2] = _diff_reg(rho)
+                reg += r3
             reg_scale = total / (reg + 1e-30)
             total = total + tikhonov_alpha * reg_scale * reg
             g_vs = g_vs + tikhonov_alpha * reg_scale * dregs[0]
             if dregs[1] is not None:
                 g_vp = g_vp + tikhonov_alpha * reg_scale * dregs[1]
+            if dregs[2] is not None:
+                g_rho = g_rho + tikhonov_alpha * reg_scale * dregs[2]
         grads = _postprocess((g_vs, g_vp, g_rho), grad_smooth_sigma, source_taper, illumination)
         return total, grads
 

@@ -239,6 +239,37 @@ class Solver:
         self._ok(self.lib.stfwi_kernel_times(self.h, out.ctypes.data), "kernel_times")
         return {k: (float(out[2 * i]), int(out[2 * i + 1])) for i, k in enumerate(self.KERNELS)}
 
+    def set_postprocess(self, grad_smooth_sigma=None, source_taper=None, illumination=None):
+        """Post-processing applied on the device to the gradients that
+        ``gradient()`` returns (fwi/gradient.py:266-277): Gaussian smoothing,
+        then the source-taper and illumination products.  None disables a
+        part; the setting stays for later calls."""
+        shp = (self.nz_dom, self.nx_dom)
+        keep = []
+        ptrs = []
+        for a in (source_taper, illumination):
+            if a is None:
+                ptrs.append(None)
+                continue
+            a = np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), shp))
+            keep.append(a)
+            ptrs.append(a.ctypes.data)
+        sigma = 0.0 if grad_smooth_sigma is None else float(grad_smooth_sigma)
+        self._ok(self.lib.stfwi_set_postprocess(self.h, sigma, ptrs[0], ptrs[1], _stream()), "set_postprocess")
+
+    def preconditioner(self, kind="illum", component=1, eps=1e-3):
+        """[nz_dom, nx_dom] FP64 gradient multiplier in [0, 1] from the forward
+        energy of the current model and shots: 'illum' (1 / (Ws + eps max Ws),
+        fwi/illumination.py:18-48) or 'eprecond3' (fwi/preconditioning.py)."""
+        k = {"illum": N.PRECOND_ILLUM, "eprecond3": N.PRECOND_EPRECOND3}.get(kind)
+        if k is None:
+            raise ValueError(f"unknown precon={kind!r}; use 'illum' or 'eprecond3'")
+        out = np.zeros((self.nz_dom, self.nx_dom), dtype=np.float64)
+        self._ok(self.lib.stfwi_preconditioner(self.h, k, int(component), float(eps), out.ctypes.data, _stream()),
+                 "preconditioner")
+        self.check()
+        return out
+
     def illumination(self, component):
         """Sum over shots and steps of field**2 on the padded grid (FP64)."""
         ws = np.zeros((self.nz, self.nx), dtype=np.float64)
@@ -246,3 +277,21 @@ class Solver:
                  "illumination")
         self.check()
         return ws
+
+
+def project_velocity_device(Vs, Vp, rho, K_margin=0.04, vp_cap=None, vs_floor=1e-3, rho_floor=1e-3):
+    """fwi/projections.py:67-117 in place on CUDA float64 tensors (torch)."""
+    import torch
+    for name, t in (("Vs", Vs), ("Vp", Vp), ("rho", rho)):
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous CUDA float64 tensor")
+    n = Vs.numel()
+    if Vp.numel() != n or rho.numel() != n:
+        raise ValueError("Vs, Vp and rho differ in size")
+    lib = N.load()
+    cap = -1.0 if vp_cap is None else float(vp_cap)
+    st = lib.stfwi_project_velocity(n, Vs.data_ptr(), Vp.data_ptr(), rho.data_ptr(), float(K_margin), cap,
+                                    float(vs_floor), float(rho_floor), _stream())
+    if st != N.STFWI_OK:
+        raise N.StfwiError(st, "stfwi_project_velocity failed")
+    return Vs, Vp, rho

@@ -25,8 +25,9 @@ def _small_case(fs=True, fd=8, nt=150):
     return vs, vp, rho, sx, sz, wav, geo
 
 
+@pytest.mark.parametrize("invert", ["vs_vp", "all"])
 @pytest.mark.parametrize("backend,ref", [("cuda", "ad"), ("cuda_imaging", "adjoint")])
-def test_compute_gradient_matches_oracle(backend, ref):
+def test_compute_gradient_matches_oracle(backend, ref, invert):
     from scipy.signal import butter
     from stfwi_b200 import fwi
     vs, vp, rho, sx, sz, wav, geo = _small_case()
@@ -37,16 +38,19 @@ def test_compute_gradient_matches_oracle(backend, ref):
     illum = 0.5 + 0.5 * np.cos(np.pi * zz / C.NZ) ** 2
     taper = np.clip(xx / 5.0, 0, 1)
     kw = dict(Vs=vs, Vp=vp, rho=rho, src_x=sx, src_z=sz, src_wavelet=wav, observed=obs, component=1,
-              invert="vs_vp", scale=3.0, sos=sos, n_taper=15, grad_smooth_sigma=1.0, source_taper=taper,
+              invert=invert, scale=3.0, sos=sos, n_taper=15, grad_smooth_sigma=1.0, source_taper=taper,
               illumination=illum, src_types=types, **geo)
     (g_vs, g_vp, g_rho), loss = fwi.compute_gradient(backend, **kw)
-    (r_vs, r_vp, _), r_loss = O.compute_gradient(ref, d0_f32=True, **kw)
+    (r_vs, r_vp, r_rho), r_loss = O.compute_gradient(ref, d0_f32=True, **kw)
     rec = O.forward_batch(vs, vp, rho, sx, sz, types, src_wavelet=wav, d0_f32=True, **geo)[:, 1]
     amp = float(np.linalg.norm(rec) / np.linalg.norm(rec - obs))
     tol = 2e-5 * max(amp, 1.0)
     errs = (abs(loss / r_loss - 1), _rel(g_vs, r_vs), _rel(g_vp, r_vp))
     assert max(errs) < tol, (errs, tol)
-    assert np.all(g_rho == 0)
+    if invert == "all":
+        assert _rel(g_rho, r_rho) < tol, (_rel(g_rho, r_rho), tol)
+    else:
+        assert np.all(g_rho == 0)
 
 
 def test_forward_and_adjoint_signatures_match_oracle():
