@@ -156,6 +156,16 @@ stfwi_status stfwi_profile(stfwi_handle *h, int32_t every);
  * Synchronises the handle's stream; resets the sums. */
 stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out);
 
+/* Tile-schedule autotuner (no counterpart in the reference): times `steps`
+ * forward and adjoint steps of the handle's configuration for several
+ * numbers of shots per block (1-8) with CUDA events around every kernel,
+ * and keeps the fastest for each of the four stencil kernels (also across
+ * later stfwi_set_shots calls); spg_out [4] (optional) receives the choice
+ * for fwd_vel, fwd_str, adj_a, adj_b.  Overwrites the fields and history:
+ * call it before the forward whose history a gradient will use.  A
+ * descriptor shot_group > 0 overrides the result.  Kernel variants 0, 2. */
+stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, void *stream);
+
 /* Residual preparation that allocates nothing (no counterpart in the
  * reference): the same misfit and adjoint sources as stfwi_misfit, without a
  * handle, for callers that cannot call cudaMalloc -- e.g. a custom call made

@@ -26,7 +26,7 @@ EXPORTS = (
     "stfwi_set_receivers", "stfwi_set_shots", "stfwi_forward", "stfwi_get_records", "stfwi_misfit",
     "stfwi_set_adjoint_sources", "stfwi_gradient", "stfwi_illumination", "stfwi_check",
     "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
-    "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity",
+    "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
 )
 
 PRECOND_ILLUM, PRECOND_EPRECOND3 = 0, 1
@@ -96,5 +96,6 @@ def load():
         L.stfwi_set_postprocess.argtypes = [H, f64, vp, vp, vp]
         L.stfwi_preconditioner.argtypes = [H, i32, i32, f64, vp, vp]
         L.stfwi_project_velocity.argtypes = [ct.c_int64, vp, vp, vp, f64, f64, f64, f64, vp]
+        L.stfwi_autotune.argtypes = [H, i32, vp, vp]
         _lib = L
     return _lib

@@ -71,6 +71,7 @@ struct stfwi_handle {
     int acc_groups = 1, acc_used = 1;
     int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
     int occ[4] = {1, 1, 1, 1};  // resident blocks per SM of fwd_vel, fwd_str, adj_a, adj_b
+    int tuned[4] = {0, 0, 0, 0};  // shots per block chosen by stfwi_autotune (0: default)
 
     // shots / receivers
     int nshot = 0;
@@ -417,8 +418,13 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
 {
     if (h->prof_every <= 0 || n % h->prof_every) return;
     const size_t idx = 2 * (size_t)(n / h->prof_every) + which;
-    // inside stream capture only an external record becomes an event node of the graph
-    if (idx < h->pev[k].size()) cudaEventRecordWithFlags(h->pev[k][idx], st, cudaEventRecordExternal);
+    // inside stream capture only an external record becomes an event node of
+    // the graph; outside (the autotuner's passes) a plain record
+    if (idx >= h->pev[k].size()) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(h->pev[k][idx], st, cudaEventRecordExternal);
+    else cudaEventRecord(h->pev[k][idx], st);
 }
 
 template <int FD>
@@ -806,6 +812,22 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
     return STFWI_OK;
 }
 
+// shots per block of each staged kernel (balanced groups; the strain phase
+// keeps at most acc_groups accumulator groups)
+void set_groups(stfwi_handle *h, const int spg_in[4])
+{
+    const int nshot = h->nshot;
+    for (int k = 0; k < 4; ++k) {
+        const int spg = std::max(1, spg_in[k]);
+        int G = (nshot + spg - 1) / spg;
+        if (k == 3) G = std::min(G, h->acc_groups);
+        h->spgk[k] = (nshot + G - 1) / G;
+        h->grp[k] = (nshot + h->spgk[k] - 1) / h->spgk[k];
+    }
+    h->acc_used = h->grp[3];
+    h->lr_used = h->grp[2];
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -1114,15 +1136,12 @@ stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
         // flight while one computes; the strain phase keeps FP64 sums per cell
         // over its shots and gains from larger groups
         static const int dflt4[4] = {3, 3, 3, 4}, dflt3[4] = {2, 2, 2, 2};
-        for (int k = 0; k < 4; ++k) {
-            const int spg = h->d.shot_group > 0 ? h->d.shot_group : (h->variant == 0 ? dflt4[k] : dflt3[k]);
-            int G = (nshot + spg - 1) / spg;
-            if (k == 3) G = std::min(G, h->acc_groups);
-            h->spgk[k] = (nshot + G - 1) / G;
-            h->grp[k] = (nshot + h->spgk[k] - 1) / h->spgk[k];
-        }
-        h->acc_used = h->grp[3];
-        h->lr_used = h->grp[2];
+        int spg[4];
+        for (int k = 0; k < 4; ++k)
+            spg[k] = h->d.shot_group > 0 ? h->d.shot_group
+                   : h->tuned[k] > 0    ? h->tuned[k]
+                                        : (h->variant == 0 ? dflt4[k] : dflt3[k]);
+        set_groups(h, spg);
     } else {
         h->acc_used = h->groups;
         h->lr_used = nshot;  // the plain U_a/V_a phase runs one shot per block row
@@ -1491,6 +1510,83 @@ stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out)
         h->prof_ms[k] = 0;
         h->prof_cnt[k] = 0;
     }
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if (h->variant == 1) return fail(h, STFWI_ERR_UNSUPPORTED, "the plain kernels run one shot per block");
+    const Geo &g = h->g;
+    steps = std::max(2, std::min((int)steps, g.nt));
+    CK(h, cudaStreamSynchronize((cudaStream_t)stream));
+    cudaStream_t st = h->hs;
+    // time `steps` forward and adjoint steps per candidate with a CUDA-event
+    // pair around every kernel (the sampled-profile records, every step)
+    const int saved_every = h->prof_every;
+    std::vector<cudaEvent_t> saved[4];
+    for (int k = 0; k < 4; ++k) {
+        saved[k].swap(h->pev[k]);
+        h->pev[k].resize(2 * (size_t)steps);
+        for (auto &e : h->pev[k]) CK(h, cudaEventCreate(&e));
+    }
+    h->prof_every = 1;
+    static const int cand[] = {1, 2, 3, 4, 5, 6, 8};
+    double best[4] = {1e300, 1e300, 1e300, 1e300};
+    int pick[4] = {h->spgk[0], h->spgk[1], h->spgk[2], h->spgk[3]};
+    stfwi_status r = STFWI_OK;
+    for (int c : cand) {
+        if (c > h->nshot) break;
+        const int spg[4] = {c, c, c, c};
+        set_groups(h, spg);
+        if ((r = zero_forward_state(h, st)) || (r = zero_adjoint_state(h, st))) break;
+        FwdOut o{};
+        o.rec = h->rec; o.status = h->status; o.slots = h->slots;
+        for (int n = 0; n < steps; ++n) fwd_step(h, n, o, st);
+        const bool ex = h->snap != nullptr;
+        for (int n = steps - 1; n >= 0; --n) {
+            AdjIn ai{};
+            ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = 0;
+            ai.accLr = h->accLr; ai.want_exact = ex && g.fs; ai.ping = n & 1;
+            AdjOut ao{};
+            ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = 0; ao.slot_img = h->slots > 1 ? 1 : -1;
+            ao.slot_next = -1; ao.accp = h->accp; ao.acc = h->acc; ao.want_exact = ex; ao.want_img = 0;
+            ao.rec_adj = h->rec_adj; ao.ping = n & 1;
+            switch (h->d.fd_order) {
+            case 2: launch_adj_step<2>(h, n, ai, ao, st); break;
+            case 4: launch_adj_step<4>(h, n, ai, ao, st); break;
+            default: launch_adj_step<8>(h, n, ai, ao, st); break;
+            }
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            r = fail(h, STFWI_ERR_CUDA, "autotune pass with %d shots per block: %s", c, cudaGetErrorString(e));
+            break;
+        }
+        for (int k = 0; k < 4; ++k) {
+            double ms = 0;
+            for (int n = 1; n < steps; ++n) {   // step 0 warms up
+                float e = 0.f;
+                if (cudaEventElapsedTime(&e, h->pev[k][2 * n], h->pev[k][2 * n + 1]) == cudaSuccess) ms += e;
+            }
+            if (ms < best[k]) { best[k] = ms; pick[k] = c; }
+        }
+    }
+    cudaGetLastError();
+    for (int k = 0; k < 4; ++k) {
+        for (cudaEvent_t e : h->pev[k]) cudaEventDestroy(e);
+        h->pev[k].swap(saved[k]);
+    }
+    h->prof_every = saved_every;
+    if (r) return r;
+    for (int k = 0; k < 4; ++k) h->tuned[k] = pick[k];
+    set_groups(h, pick);
+    drop_graphs(h);
+    h->stored = false;   // the timing passes overwrote the state
+    if (spg_out)
+        for (int k = 0; k < 4; ++k) spg_out[k] = pick[k];
     return STFWI_OK;
 }
 

@@ -239,6 +239,14 @@ class Solver:
         self._ok(self.lib.stfwi_kernel_times(self.h, out.ctypes.data), "kernel_times")
         return {k: (float(out[2 * i]), int(out[2 * i + 1])) for i, k in enumerate(self.KERNELS)}
 
+    def autotune(self, steps=20):
+        """Pick the shots per block of each stencil kernel by timing `steps`
+        forward and adjoint steps per candidate; returns {kernel: shots per
+        block}.  Overwrites the state: call before the forward of a gradient."""
+        out = np.zeros(4, dtype=np.int32)
+        self._ok(self.lib.stfwi_autotune(self.h, int(steps), out.ctypes.data, _stream()), "autotune")
+        return dict(zip(self.KERNELS, (int(v) for v in out)))
+
     def set_postprocess(self, grad_smooth_sigma=None, source_taper=None, illumination=None):
         """Post-processing applied on the device to the gradients that
         ``gradient()`` returns (fwi/gradient.py:266-277): Gaussian smoothing,

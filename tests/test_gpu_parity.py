@@ -340,3 +340,35 @@ def test_density_gradient_checkpointed_equals_store_all():
         S.close()
     for a, b in zip(out[1], out[0]):
         assert _rel(a, b) < 1e-12, _rel(a, b)
+
+
+def test_autotuned_schedule_gives_the_same_gradient():
+    """stfwi_autotune picks shots per block for each kernel by timing; the
+    gradient computed with the tuned schedule equals the default schedule's
+    (the grouping only changes the summation order of a launch's shots)."""
+    vs, vp, rho = C.model()
+    nt, fd, fs = 90, 8, True
+    rx = np.arange(1, C.NX - 1, 3, dtype=np.int32)
+    rz = np.ones_like(rx)
+    sx = np.array([3, 7, 11, 15, 19, 23, 27])
+    sz = np.array([2, 5, 3, 6, 2, 4, 3])
+    types = ["force", "moment"] * 3 + ["force"]
+    wav = (O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9).astype(np.float32)
+    obs = np.random.default_rng(5).standard_normal((7, nt, len(rx))).astype(np.float32) * 1e-9
+    res = []
+    for tune in (False, True):
+        S = _solver(nt, len(rx), 7, fd, fs, want_gradient=True)
+        S.set_model(vs, vp, rho)
+        S.set_receivers(rx, rz)
+        S.set_shots(sx, sz, types, wav)
+        if tune:
+            pick = S.autotune(steps=10)
+            assert set(pick) == {"fwd_vel", "fwd_str", "adj_a", "adj_b"}
+            assert all(v in (1, 2, 3, 4, 5, 6, 8) for v in pick.values()), pick
+        S.forward(store=True)
+        mis = S.misfit(obs, 1, 1.0)
+        g = S.gradient(exact=True, imaging=True)
+        res.append((mis, g["exact"][0], g["imaging"][0]))
+        S.close()
+    for a, b in zip(res[1], res[0]):
+        assert _rel(a, b) < 1e-6, _rel(a, b)
