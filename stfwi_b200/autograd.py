@@ -10,7 +10,8 @@ misfit) into the forward and returns the scalar loss.
 
 A solver keeps the history of its last storing forward only: a backward
 must follow its own forward before the solver runs another one (checked).
-The density gradient is not accumulated; inputs with rho.requires_grad raise.
+The density gradient needs a solver made with density=True (it keeps the
+velocities in the history); otherwise rho.requires_grad raises.
 """
 from __future__ import annotations
 
@@ -23,8 +24,8 @@ from .solver import Solver
 def _check(solver, rho):
     if not isinstance(solver, Solver):
         raise TypeError("solver must be a stfwi_b200.Solver")
-    if rho.requires_grad:
-        raise NotImplementedError("the density gradient is not accumulated on the GPU")
+    if rho.requires_grad and not getattr(solver, "density", False):
+        raise NotImplementedError("the density gradient needs a Solver created with density=True")
 
 
 class _Forward(torch.autograd.Function):
@@ -34,7 +35,7 @@ class _Forward(torch.autograd.Function):
         solver.set_model(vs, vp, rho)
         solver.forward(store=True)
         solver._version = getattr(solver, "_version", 0) + 1
-        ctx.solver, ctx.version, ctx.dtypes = solver, solver._version, (vs.dtype, vp.dtype)
+        ctx.solver, ctx.version, ctx.dtypes = solver, solver._version, (vs.dtype, vp.dtype, rho.dtype)
         out = torch.empty((solver.nshot, 4, solver.nt, solver.nrec), dtype=torch.float32, device=vs.device)
         solver.records(out=out)
         return out
@@ -47,7 +48,8 @@ class _Forward(torch.autograd.Function):
         S.set_adjoint_sources(grad_rec.detach().to(torch.float32).contiguous())
         g = torch.empty((1, 3, S.nz_dom, S.nx_dom), dtype=torch.float64, device=grad_rec.device)
         S.gradient(exact=True, out=g)
-        return g[0, 0].to(ctx.dtypes[0]), g[0, 1].to(ctx.dtypes[1]), None, None
+        grho = g[0, 2].to(ctx.dtypes[2]) if S.density else None
+        return g[0, 0].to(ctx.dtypes[0]), g[0, 1].to(ctx.dtypes[1]), grho, None
 
 
 class _Misfit(torch.autograd.Function):
@@ -59,7 +61,7 @@ class _Misfit(torch.autograd.Function):
         solver._version = getattr(solver, "_version", 0) + 1
         mis = torch.zeros(solver.nshot, dtype=torch.float64, device=vs.device)
         solver.misfit(observed, component, scale, sos, n_taper, nshot_norm=nshot_norm, out=mis)
-        ctx.solver, ctx.version, ctx.dtypes = solver, solver._version, (vs.dtype, vp.dtype)
+        ctx.solver, ctx.version, ctx.dtypes = solver, solver._version, (vs.dtype, vp.dtype, rho.dtype)
         return mis.sum()
 
     @staticmethod
@@ -69,8 +71,9 @@ class _Misfit(torch.autograd.Function):
             raise RuntimeError("the solver ran another forward before this backward")
         g = torch.empty((1, 3, S.nz_dom, S.nx_dom), dtype=torch.float64, device=gout.device)
         S.gradient(exact=True, out=g)
-        return ((gout * g[0, 0]).to(ctx.dtypes[0]), (gout * g[0, 1]).to(ctx.dtypes[1]),
-                None, None, None, None, None, None, None, None)
+        grho = (gout * g[0, 2]).to(ctx.dtypes[2]) if S.density else None
+        return ((gout * g[0, 0]).to(ctx.dtypes[0]), (gout * g[0, 1]).to(ctx.dtypes[1]), grho,
+                None, None, None, None, None, None, None)
 
 
 def elastic_forward(vs, vp, rho, solver):

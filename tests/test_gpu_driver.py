@@ -177,3 +177,40 @@ def test_multiscale_driver_matches_oracle_driven_run(monkeypatch):
         print(f"stage {a['stage']}: {n} evaluations, loss rel diff {err:.2e}, {la[0]:.4e} -> {la[n - 1]:.4e}")
         assert err < 1e-3, err
     assert h_gpu[-1]["loss_history"].min() < 0.9 * h_gpu[0]["loss_history"][0]
+
+
+def test_uneven_batch_equals_models_run_alone():
+    """Two grids of different size and step count, their launches
+    interleaved on two streams (stfwi_b200.batch.UnevenBatch), give each
+    model's own misfit and gradient."""
+    import torch
+    from stfwi_b200 import Solver
+    from stfwi_b200 import models as Mo
+    from stfwi_b200.batch import UnevenBatch
+    specs = []
+    for nz, nx, dx, nt, ns, fd in ((40, 90, 20.0, 120, 3, 4), (64, 150, 10.0, 200, 4, 8)):
+        vs, vp, rho = Mo.layered_fault_model(nz, nx, seed=3)
+        dt = 1.5e-3 * dx / 20.0
+        specs.append(dict(nz_dom=nz, nx_dom=nx, dx=dx, dz=dx, dt=dt, nt=nt, fc=12.0, pad=10, fd_order=fd,
+                          free_surface=True, src_x=np.linspace(5, nx - 6, ns).astype(np.int64),
+                          src_z=np.full(ns, 2), src_types=["force", "moment"] * (ns // 2) + ["force"] * (ns % 2),
+                          wavelet=Mo.ricker(np.arange(nt) * dt, 12.0, 1.5 / 12.0), rec_x=np.arange(0, nx, 3),
+                          rec_z=np.ones(len(range(0, nx, 3)), dtype=np.int64), mem_budget_gb=4.0,
+                          true=(vs, vp, rho), init=Mo.smooth_initial(vs, vp, rho, 4.0)))
+    B = UnevenBatch(specs)
+    obs = [r[:, 1].contiguous() for r in B.records([s["true"] for s in specs])]
+    res = B.gradient([s["init"] for s in specs], obs)
+    B.close()
+    for s, o, (mis, g) in zip(specs, obs, res):
+        S = Solver(s["nz_dom"], s["nx_dom"], s["dx"], s["dz"], s["dt"], s["nt"], s["fc"], s["pad"], len(s["rec_x"]),
+                   len(s["src_x"]), fd_order=s["fd_order"], free_surface=True, want_gradient=True)
+        S.set_receivers(s["rec_x"], s["rec_z"])
+        S.set_shots(s["src_x"], s["src_z"], s["src_types"], np.asarray(s["wavelet"], dtype=np.float32))
+        S.set_model(*s["init"])
+        S.forward(store=True)
+        m1 = S.misfit(o, 1, 1.0)
+        g1 = S.gradient(exact=True)["exact"]
+        S.close()
+        assert _rel(mis.cpu().numpy(), m1) < 1e-12
+        for c in range(2):
+            assert _rel(g[c].cpu().numpy(), g1[c]) < 1e-12, c
