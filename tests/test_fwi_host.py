@@ -1,5 +1,6 @@
 """Host-side pieces of the reference-signature API (CPU)."""
 import numpy as np
+import pytest
 
 from oracle import oracle as O
 
@@ -40,3 +41,44 @@ def test_layered_fault_model_ranges():
     # config 1 / 2 are stable: CFL number below 1
     for cfg in (Mo.CONFIG1, Mo.CONFIG2):
         assert Mo.cfl_number(4700, cfg["dt"], cfg["dx"], cfg["dz"], cfg["fd_order"]) < 0.7
+
+
+def test_host_projection_matches_oracle_and_reference_rules():
+    """fwi/projections.py:67-117: Vp capped first, then Vs <= Vp / r, floors."""
+    from oracle import oracle as O
+    from stfwi_b200 import fwi
+    rng = np.random.default_rng(4)
+    vs = rng.uniform(-10.0, 3000.0, (20, 30))
+    vp = rng.uniform(100.0, 5000.0, (20, 30))
+    rho = rng.uniform(-1.0, 2500.0, (20, 30))
+    for cap in (None, 4000.0):
+        got = fwi.project_velocity(vs, vp, rho, K_margin=0.04, vp_cap=cap)
+        ref = O.project_velocity(vs, vp, rho, K_margin=0.04, vp_cap=cap)
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
+        r = fwi.k_safe_ratio(0.04)
+        above_floor = got[0] > 1e-3
+        assert np.all(got[0][above_floor] <= got[1][above_floor] / r)
+        assert np.all(got[0] >= 1e-3) and np.all(got[2] >= 1e-3)
+        if cap is not None:
+            assert np.all(got[1] <= cap)
+    assert abs(fwi.k_safe_ratio(0.0) - 2 / np.sqrt(3)) < 1e-15
+    assert fwi.cfl_vp_cap(20.0, 10.0, 1e-3, 0.5) == 0.5 * 10.0 / 1e-3
+
+
+def test_driver_plateau_and_block_helpers():
+    """The stage helpers of fwi/optim_lbfgsb.py: plateau window, active
+    blocks, block scales."""
+    from stfwi_b200.fwi import optim_lbfgsb as D
+    p = D._Plateau(3, 1e-3)
+    stops = [p.push(v) for v in (10, 9, 8, 7, 6, 5)]   # still dropping: no stop
+    assert stops == [False] * 6
+    q = D._Plateau(3, 1e-3)
+    stops = [q.push(v) for v in (5.0, 5.0, 5.0, 5.0, 5.0, 4.999)]   # last 3 vs previous 3 within 0.1 %
+    assert stops == [False] * 5 + [True]
+    assert D._Plateau(None, 1e-3).push(1.0) is False
+    assert D._active_keys("vs") == ["Vs"] and D._active_keys("all") == ["Vs", "Vp", "rho"]
+    with pytest.raises(ValueError):
+        D._active_keys("rho")
+    s = D._block_scales((np.array([[-3.0, 2.0]]), np.zeros((1, 2)), np.array([[1.0, 5.0]])))
+    assert s == [3.0, 1e-12, 5.0]
