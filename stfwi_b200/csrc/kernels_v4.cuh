@@ -56,7 +56,9 @@ template <int FD> struct L4 {
     static constexpr int TABB = al32_3(5 * SW4 + 4 * B::SH);
     static constexpr int ADA_STAGE = A::S3 + OWN2;   // + P, Q of the own cells
     static constexpr int ADA = 2 * ADA_STAGE + A::S1 + TABA;
-    static constexpr int ADB = 2 * B::S2 + 2 * B::S1 + TABB;
+    static constexpr int OWNB3 = al32_3(3 * B::TZH * TX4);   // strain adjoints of the own cells
+    static constexpr int ADB_STAGE = B::S2 + OWNB3;
+    static constexpr int ADB = 2 * ADB_STAGE + 2 * B::S1 + TABB;
     static constexpr size_t bytes(int floats, int nbar) { return (size_t)floats * 4 + 8 * nbar; }
 };
 
@@ -889,13 +891,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 template <int FD, bool EXACT, bool IMG, bool RHO>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
-             AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ)
+             AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ,
+             const __grid_constant__ CUtensorMap tmEo)
 {
     using T = G4<FD, RPT4B>;
     constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4B;
+    constexpr int STG = L4<FD>::ADB_STAGE, OWNB = 3 * T::TZH * TX4 * 4, PL = T::TZH * TX4;
     extern __shared__ __align__(128) float sm[];
     constexpr int NCC = (SW4 + TX - 1) / TX;
-    float *aZXZ = sm + 2 * T::S2, *aXXZ = aZXZ + T::S1;
+    float *aZXZ = sm + 2 * STG, *aXXZ = aZXZ + T::S1;
     float *tab = aXXZ + T::S1;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L4<FD>::ADB);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -906,8 +910,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
         fence_async_shared();
         for (int b = 0; b < 2 && b < nsh; ++b) {
-            mbar_arrive_expect_tx(bar + b, 2 * SN * 4);
-            tma_load_4d(sm + b * T::S2, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+            mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB);
+            tma_load_4d(sm + b * STG, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
+            tma_load_4d(sm + b * STG + T::S2, &tmEo, bar + b, c.j0, c.i0, F_EX, c.s0 + b);
         }
     }
     __syncthreads();
@@ -956,7 +961,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
     for (int it = 0; it < nsh; ++it) {
         const int s = c.s0 + it;
-        float *S = sm + (it & 1) * T::S2;
+        float *S = sm + (it & 1) * STG;
+        const float *own = S + T::S2;   // [ex_a, ez_a, es_a][TZH][TX4] of the tile's own cells
         float *exa = A + ((long long)s * F_N + F_EX) * g.fstride;
         float *eza = A + ((long long)s * F_N + F_EZ) * g.fstride;
         float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
@@ -1057,14 +1063,11 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int i = c.i0 + ty * RPT + r;
             if (!LEAN && i >= g.nz) continue;
             const int q = (ty * RPT + r + K) * SW4 + XO4 + 2 * tx;
-            float ea[2] = {0.f, 0.f}, za[2] = {0.f, 0.f}, sa[2] = {0.f, 0.f};
-            if (jb < g.nx) {
-                const long long off = (long long)i * g.P + jb;
-                const float2 a = *reinterpret_cast<const float2 *>(exa + off);
-                const float2 b = *reinterpret_cast<const float2 *>(eza + off);
-                const float2 d = *reinterpret_cast<const float2 *>(esa + off);
-                ea[0] = a.x; ea[1] = a.y; za[0] = b.x; za[1] = b.y; sa[0] = d.x; sa[1] = d.y;
-            }
+            const int qo = (ty * RPT + r) * TX4 + 2 * tx;
+            const float2 a2 = *reinterpret_cast<const float2 *>(own + qo);
+            const float2 b2 = *reinterpret_cast<const float2 *>(own + PL + qo);
+            const float2 d2 = *reinterpret_cast<const float2 *>(own + 2 * PL + qo);
+            const float ea[2] = {a2.x, a2.y}, za[2] = {b2.x, b2.y}, sa[2] = {d2.x, d2.y};
             float axx[10], axz[10];
             xrow(axx, aXX, q);
             xrow(axz, sXXZ, q);
@@ -1189,8 +1192,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
-            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4);
+            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB);
             tma_load_4d(S, &tmPQ, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
+            tma_load_4d(S + T::S2, &tmEo, bar + (it & 1), c.j0, c.i0, F_EX, s + 2);
         }
         if (n > 0) {
             const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];

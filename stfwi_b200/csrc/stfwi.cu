@@ -59,7 +59,7 @@ struct stfwi_handle {
     int variant = 0, sms = 148;
     int accp = 5;   // accumulator planes per shot group (7 with the density terms)
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
-    CUtensorMap tmUo{}, tmSo{}, tmPQo{};   // own-cell boxes of the two-column kernels
+    CUtensorMap tmUo{}, tmSo{}, tmPQo{}, tmEo{};   // own-cell boxes of the two-column kernels
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
     // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
     // variant 2: 32 x 8*RPT3 and 32 x 32)
@@ -543,7 +543,7 @@ void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, 
     auto launch = [&](auto kern) {
         kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L4<FD>::bytes(L4<FD>::ADB, 2), st>>>(
             h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
-            h->tmPQ);
+            h->tmPQ, h->tmEo);
     };
     const bool rho = h->g.snf == 5;
     if (ao.want_exact && ao.want_img) rho ? launch(k4_adj_b<FD, true, true, true>) : launch(k4_adj_b<FD, true, true, false>);
@@ -782,6 +782,12 @@ stfwi_status setup_tma_kernels(stfwi_handle *h)
     if (r) return r;
     CK(h, cudaFuncSetAttribute((const void *)k4_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)L4<FD>::bytes(L4<FD>::STR, 2)));
+    // the density-gradient instantiations of the strain phase
+    const void *const rho_kern[3] = {(const void *)k4_adj_b<FD, true, false, true>,
+                                     (const void *)k4_adj_b<FD, true, true, true>,
+                                     (const void *)k4_adj_b<FD, false, true, true>};
+    for (const void *k : rho_kern)
+        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L4<FD>::bytes(L4<FD>::ADB, 2)));
     return STFWI_OK;
 }
 
@@ -808,6 +814,8 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
         if ((r = encode(h, &h->tmUo, h->F, 4, fdims, fstr, own2))) return r;
         if ((r = encode(h, &h->tmSo, h->F, 4, fdims, fstr, own3))) return r;
         if ((r = encode(h, &h->tmPQo, h->A, 4, fdims, fstr, own2))) return r;
+        const cuuint32_t own3b[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->thb, 3, 1};
+        if ((r = encode(h, &h->tmEo, h->A, 4, fdims, fstr, own3b))) return r;
     }
     return STFWI_OK;
 }

@@ -19,17 +19,19 @@ import numpy as np
 def specs(scale=1.0):
     from . import models as Mo
     out = []
+    # memory budgets (GB): store-all history for the small grid, checkpoint
+    # segments chosen by the handle for the two larger ones (180 GB in all)
     for (nz, nx, dx, nt, ns, fc, fd, budget) in ((152, 500, 20.0, 2000, 8, 5.0, 4, 16.0),
-                                                 (304, 1000, 10.0, 4000, 16, 10.0, 8, 24.0),
-                                                 (608, 2000, 5.0, 8000, 32, 15.0, 8, 115.0)):
+                                                 (304, 1000, 10.0, 4000, 16, 10.0, 8, 14.0),
+                                                 (608, 2000, 5.0, 8000, 32, 15.0, 8, 128.0)):
         nt = max(50, int(nt * scale))
         dt = 1.5e-3 * dx / 20.0
         vs, vp, rho = Mo.layered_fault_model(nz, nx, seed=11)
         sx = np.linspace(nx // 20, nx - nx // 20 - 1, ns).astype(np.int64)
         out.append(dict(nz_dom=nz, nx_dom=nx, dx=dx, dz=dx, dt=dt, nt=nt, fc=fc, pad=20, fd_order=fd,
                         free_surface=True, src_x=sx, src_z=np.full(ns, 2), src_types=["force", "moment"] * (ns // 2),
-                        wavelet=Mo.ricker(np.arange(nt) * dt, fc, 1.5 / fc), rec_x=np.arange(0, nx, 2),
-                        rec_z=np.ones(nx // 2, dtype=np.int64), mem_budget_gb=budget,
+                        wavelet=Mo.ricker(np.arange(nt) * dt, fc, 1.5 / fc), rec_x=np.arange(0, nx, 4),
+                        rec_z=np.ones(nx // 4, dtype=np.int64), mem_budget_gb=budget,
                         true=(vs, vp, rho), init=Mo.smooth_initial(vs, vp, rho, 10.0)))
     return out
 

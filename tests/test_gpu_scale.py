@@ -83,9 +83,9 @@ def test_gradient_at_scale_vs_finite_differences():
         S.forward()
         return float(S.misfit(obs, 1, scale, sos, n_taper).sum())
 
-    # FP32 traces make the misfit itself noisy at ~1e-7 of its value (the
+    # FP32 traces make the misfit itself noisy at ~1e-6 of its value (the
     # rounding differs between two nearby models): each comparison allows
-    # 1 % of <g, d> plus that floor, 5e-7 J, divided by the step 2h
+    # 1 % of <g, d> plus that floor, 2e-6 J, divided by the step 2h
     J = float(loss)
     rng = np.random.default_rng(2026)
     worst = 0.0
@@ -94,7 +94,7 @@ def test_gradient_at_scale_vs_finite_differences():
         h = 20.0 / np.abs(d).max()   # at most 20 m/s (about 1 % of Vs)
         fd = (misfit(init[0] + h * d) - misfit(init[0] - h * d)) / (2 * h)
         an = float(np.sum(g * d))
-        allow = 1e-2 * abs(an) + 5e-7 * J / (2 * h)
+        allow = 1e-2 * abs(an) + 2e-6 * J / (2 * h)
         worst = max(worst, abs(fd - an) / allow)
         print(f"perturbation {k:2d}: FD {fd:+.6e}  <g, d> {an:+.6e}  rel {abs(fd - an) / abs(an):.2e}  "
               f"(error / allowance {abs(fd - an) / allow:.2f})")
@@ -131,17 +131,19 @@ def test_dot_product_identity_at_scale():
 
 
 def test_short_gradient_at_scale_vs_oracle():
-    """Two shots, 150 steps on the full grid: the exact gradient against the
-    FP64 oracle."""
+    """Two shots, 300 steps on the full grid: the traces and the exact
+    gradient against the FP64 oracle (observed data from Vs x 1.05, so that
+    the residual is not a difference of nearly equal traces)."""
     from stfwi_b200 import Solver
     from stfwi_b200 import models as Mo
-    nt = 150
+    nt = 300
     true, init, _, _, _, rx, rz = _geometry(2)
     sx, sz, types = np.array([700, 1300]), np.array([4, 30]), ["force", "moment"]
-    wav = Mo.ricker(np.arange(nt) * DT, FC, 1.5 / FC)
+    wav = Mo.ricker(np.arange(nt) * DT, FC, 0.06)
     geo = dict(rec_x=rx, rec_z=rz, nx_dom=NX, nz_dom=NZ, dx=DX, dz=DX, dt=DT, nt=nt, fc=FC, pad=PAD,
                fd_order=FD, free_surface=True, d0_f32=True)
-    obs = O.forward_batch(*true, sx, sz, types, src_wavelet=wav, **geo)[:, 1]
+    ref_rec = O.forward_batch(*init, sx, sz, types, src_wavelet=wav, **geo)
+    obs = O.forward_batch(init[0] * 1.05, init[1], init[2], sx, sz, types, src_wavelet=wav, **geo)[:, 1]
     kw = dict(src_x=sx, src_z=sz, src_wavelet=wav, observed=obs, src_types=types, component=1, scale=1.0,
               invert="vs", **geo)
     (g_ref, _, _), loss = O.compute_gradient("ad", Vs=init[0], Vp=init[1], rho=init[2], **kw)
@@ -150,9 +152,15 @@ def test_short_gradient_at_scale_vs_oracle():
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav.astype(np.float32))
     S.forward(store=True)
+    rec = S.records()
     mis = S.misfit(obs.astype(np.float32), 1, 1.0)
     g = S.gradient(exact=True)["exact"][0]
     S.close()
+    amp = float(np.linalg.norm(rec[:, 1]) / np.linalg.norm(rec[:, 1] - obs))
+    e_rec = max(_rel(rec[k, c], ref_rec[k, c]) for k in range(2) for c in range(4))
     e = (abs(mis.sum() / loss - 1), _rel(g, g_ref))
-    print(f"short run on the full grid: misfit rel {e[0]:.2e}, g_Vs rel-L2 {e[1]:.2e}")
-    assert e[0] < 1e-4 and e[1] < 1e-4, e
+    print(f"short run on the full grid: traces rel-L2 {e_rec:.2e}, amplification {amp:.1f}, "
+          f"misfit rel {e[0]:.2e}, g_Vs rel-L2 {e[1]:.2e}")
+    assert e_rec < 1e-5, e_rec
+    tol = 2e-5 * max(amp, 1.0)
+    assert e[0] < tol and e[1] < tol, (e, tol)
