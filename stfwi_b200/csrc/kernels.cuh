@@ -532,6 +532,7 @@ struct AdjOut {
     float *src_a;          // [nshot][nt] or null
     const float *rec_adj;  // [nshot][4][nt][nrec]
     int ping;
+    int hist_tma;          // two-column kernels: the carry-in stresses arrive by TMA (history map valid)
 };
 
 template <int FD, bool EXACT, bool IMG>

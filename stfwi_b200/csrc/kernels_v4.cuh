@@ -57,7 +57,8 @@ template <int FD> struct L4 {
     static constexpr int ADA_STAGE = A::S3 + OWN2;   // + P, Q of the own cells
     static constexpr int ADA = 2 * ADA_STAGE + A::S1 + TABA;
     static constexpr int OWNB3 = al32_3(3 * B::TZH * TX4);   // strain adjoints of the own cells
-    static constexpr int ADB_STAGE = B::S2 + OWNB3;
+    // + the carry-in stresses of the own cells from the history (exact gradient)
+    static constexpr int ADB_STAGE = B::S2 + 2 * OWNB3;
     static constexpr int ADB = 2 * ADB_STAGE + 2 * B::S1 + TABB;
     static constexpr size_t bytes(int floats, int nbar) { return (size_t)floats * 4 + 8 * nbar; }
 };
@@ -892,7 +893,7 @@ template <int FD, bool EXACT, bool IMG, bool RHO>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     k4_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
              AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ,
-             const __grid_constant__ CUtensorMap tmEo)
+             const __grid_constant__ CUtensorMap tmEo, const __grid_constant__ CUtensorMap tmH)
 {
     using T = G4<FD, RPT4B>;
     constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4B;
@@ -906,13 +907,20 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
     const int nsh = c.s1 - c.s0;
     if (nsh <= 0) return;
+    // the carry-in stresses of the exact gradient: one more box per shot from
+    // the history [shot][slot * snf + field][nz_dom][nx_dom] at the tile's
+    // physical coordinates (cells outside the physical domain arrive as 0)
+    const bool htma = EXACT && o.hist_tma && o.slot_in >= 0;
+    const int hbytes = htma ? OWNB : 0;
+    const int hx = c.j0 - g.pad, hy = c.i0 - g.z0, hz = o.slot_in * g.snf;
     if (tid == 0) {
         mbar_init(bar + 0, 1); mbar_init(bar + 1, 1);
         fence_async_shared();
         for (int b = 0; b < 2 && b < nsh; ++b) {
-            mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB);
+            mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(sm + b * STG, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
             tma_load_4d(sm + b * STG + T::S2, &tmEo, bar + b, c.j0, c.i0, F_EX, c.s0 + b);
+            if (htma) tma_load_4d(sm + b * STG + T::S2 + L4<FD>::OWNB3, &tmH, bar + b, hx, hy, hz, c.s0 + b);
         }
     }
     __syncthreads();
@@ -924,11 +932,16 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     bool colin[2];
     colin[0] = jb >= T::M && jb <= g.nx - 1 - T::M;
     colin[1] = jb + 1 >= T::M && jb + 1 <= g.nx - 1 - T::M;
-    float mL2M[RPT][2], mL[RPT][2], mM2[RPT][2], idet[RPT][2], i2m[RPT][2];
     constexpr int RE = EXACT ? RPT : 1, RI = IMG ? RPT : 1;
+    float mL2M[RPT][2], mL[RPT][2], mM2[RPT][2], idet[RI][2], i2m[RI][2];
     // per-launch sums over the block's shots (at most a few terms) in FP32;
-    // the sums over steps and shot groups are FP64 (the reductions below)
-    float gM[RE][2], gL[RE][2], gL2M[RE][2], glam[RI][2], gmu[RI][2];
+    // the sums over steps and shot groups are FP64 (the reductions below).
+    // The exact gradient sums the carry-in stresses s against the stress
+    // adjoints, sA = sum(s1 sxx_a + s2 szz_a), sB = sum(s2 sxx_a + s1 szz_a),
+    // sC = sum(s3 sxz_a); the strain-recovery factors (constant per cell)
+    // are applied once at the end: g_L2M = idet (L2M sA - L sB), g_L =
+    // idet (L2M sB - L sA), g_M = sC / M.
+    float sC[RE][2], sB[RE][2], sA[RE][2], glam[RI][2], gmu[RI][2];
     // density terms (history with velocities): dJ/dB of the exact gradient
     // and the rho term of the imaging formula
     constexpr int RB = (EXACT && RHO) ? RPT : 1, RR = (IMG && RHO) ? RPT : 1;
@@ -947,13 +960,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             mL2M[r][cc] = inb ? m.L2M[off] : 0.f;
             mL[r][cc] = inb ? m.L[off] : 0.f;
             mM2[r][cc] = inb ? 2.f * m.M[off] : 0.f;
-            idet[r][cc] = inb ? 1.0f / ((mL2M[r][cc] - mL[r][cc]) * (mL2M[r][cc] + mL[r][cc])) : 0.f;
-            i2m[r][cc] = inb ? 1.0f / mM2[r][cc] : 0.f;
+            if (IMG) {
+                idet[r % RI][cc] = inb ? 1.0f / ((mL2M[r][cc] - mL[r][cc]) * (mL2M[r][cc] + mL[r][cc])) : 0.f;
+                i2m[r % RI][cc] = inb ? 1.0f / mM2[r][cc] : 0.f;
+            }
         }
 #pragma unroll
     for (int r = 0; r < RE; ++r)
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) gM[r][cc] = gL[r][cc] = gL2M[r][cc] = 0.f;
+        for (int cc = 0; cc < 2; ++cc) sC[r][cc] = sB[r][cc] = sA[r][cc] = 0.f;
 #pragma unroll
     for (int r = 0; r < RI; ++r)
 #pragma unroll
@@ -963,6 +978,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         const int s = c.s0 + it;
         float *S = sm + (it & 1) * STG;
         const float *own = S + T::S2;   // [ex_a, ez_a, es_a][TZH][TX4] of the tile's own cells
+        const float *hown = own + L4<FD>::OWNB3;   // [sxx, szz, sxz][TZH][TX4] carry-in (htma)
         float *exa = A + ((long long)s * F_N + F_EX) * g.fstride;
         float *eza = A + ((long long)s * F_N + F_EZ) * g.fstride;
         float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
@@ -1073,7 +1089,12 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             xrow(axz, sXXZ, q);
             const bool rowin = i >= T::M && i <= g.nz - 1 - T::M;
             float h1[2] = {0.f, 0.f}, h2[2] = {0.f, 0.f}, h3[2] = {0.f, 0.f};
-            if (EXACT && snap_in) {
+            if (EXACT && htma) {
+                const float2 x1 = *reinterpret_cast<const float2 *>(hown + qo);
+                const float2 x2 = *reinterpret_cast<const float2 *>(hown + PL + qo);
+                const float2 x3 = *reinterpret_cast<const float2 *>(hown + 2 * PL + qo);
+                h1[0] = x1.x; h1[1] = x1.y; h2[0] = x2.x; h2[1] = x2.y; h3[0] = x3.x; h3[1] = x3.y;
+            } else if (EXACT && snap_in) {
 #pragma unroll
                 for (int cc = 0; cc < 2; ++cc) {
                     const int pi = i - g.z0, pj = jb + cc - g.pad;
@@ -1116,11 +1137,18 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     } else {
                         if (o.src_a) o.src_a[(long long)s * g.nt + n] = (g.dt / sh.mcoef[s]) * (ea[cc] + za[cc]);
                         if (EXACT) {
+                            // the moment factor's (L + M) term, straight into
+                            // this group's FP64 sums of the source cell
                             const double lm = sh.lm[s];
                             const double glm = -((double)w * g.dt / ((double)sh.mcoef[s] / lm)) / (lm * lm)
                                                * (double)(ea[cc] + za[cc]);
-                            gM[r % RE][cc] += (float)glm;
-                            gL[r % RE][cc] += (float)glm;
+                            const int pi = i - g.z0, pj = j - g.pad;
+                            if (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
+                                double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd +
+                                              (long long)pi * g.nx_dom + pj;
+                                atomicAdd(acc, glm);
+                                atomicAdd(acc + g.nd, glm);
+                            }
                         }
                     }
                 }
@@ -1128,12 +1156,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 nez[cc] = za[cc] + mL[r][cc] * sxx + mL2M[r][cc] * szz;
                 nes[cc] = sa[cc] + mM2[r][cc] * sxz;
                 if (EXACT) {
-                    const float e1 = (mL2M[r][cc] * h1[cc] - mL[r][cc] * h2[cc]) * idet[r][cc];
-                    const float e2 = (mL2M[r][cc] * h2[cc] - mL[r][cc] * h1[cc]) * idet[r][cc];
-                    const float e3 = h3[cc] * i2m[r][cc];
-                    gL2M[r % RE][cc] += e1 * sxx + e2 * szz;
-                    gL[r % RE][cc] += e2 * sxx + e1 * szz;
-                    gM[r % RE][cc] += 2.f * e3 * sxz;
+                    sA[r % RE][cc] += h1[cc] * sxx + h2[cc] * szz;
+                    sB[r % RE][cc] += h2[cc] * sxx + h1[cc] * szz;
+                    sC[r % RE][cc] += h3[cc] * sxz;
                 }
                 const int pi = i - g.z0, pj = j - g.pad;
                 if (RHO && (LEAN || (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom))) {
@@ -1168,9 +1193,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     const float dzBU = (Pp[ozp] - Pp[ozm]) * g.inv2dz;
                     const float dxBV = (Qp[oxp] - Qp[oxm]) * g.inv2dx;
                     const float t1 = snap_img[pq], t2 = snap_img[g.nd + pq], t3 = snap_img[2 * g.nd + pq];
-                    const float e1 = (mL2M[r][cc] * t1 - mL[r][cc] * t2) * idet[r][cc];
-                    const float e2 = (mL2M[r][cc] * t2 - mL[r][cc] * t1) * idet[r][cc];
-                    const float e3 = t3 * i2m[r][cc];
+                    const float e1 = (mL2M[r][cc] * t1 - mL[r][cc] * t2) * idet[r % RI][cc];
+                    const float e2 = (mL2M[r][cc] * t2 - mL[r][cc] * t1) * idet[r % RI][cc];
+                    const float e3 = t3 * i2m[r % RI][cc];
                     glam[r % RI][cc] -= g.dt * ((e1 + e2) * (dxBU + dzBV));
                     gmu[r % RI][cc] -= g.dt * (2.f * e1 * dxBU + 2.f * e2 * dzBV + e3 * (dzBU + dxBV));
                 }
@@ -1192,9 +1217,10 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         fence_async_shared();
         __syncthreads();
         if (tid == 0 && it + 2 < nsh) {
-            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB);
+            mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(S, &tmPQ, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
             tma_load_4d(S + T::S2, &tmEo, bar + (it & 1), c.j0, c.i0, F_EX, s + 2);
+            if (htma) tma_load_4d(S + T::S2 + L4<FD>::OWNB3, &tmH, bar + (it & 1), hx, hy, hz, s + 2);
         }
         if (n > 0) {
             const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
@@ -1219,9 +1245,12 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     // launch: the atomic adds only avoid waiting for the loads
                     double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
                     if (EXACT) {
-                        atomicAdd(acc, (double)gM[r % RE][cc]);
-                        atomicAdd(acc + g.nd, (double)gL[r % RE][cc]);
-                        atomicAdd(acc + 2 * g.nd, (double)gL2M[r % RE][cc]);
+                        const double l2m = mL2M[r][cc], l = mL[r][cc];
+                        const double id = 1.0 / ((l2m - l) * (l2m + l));
+                        const double a = sA[r % RE][cc], b = sB[r % RE][cc];
+                        atomicAdd(acc, 2.0 * (double)sC[r % RE][cc] / (double)mM2[r][cc]);
+                        atomicAdd(acc + g.nd, id * (l2m * b - l * a));
+                        atomicAdd(acc + 2 * g.nd, id * (l2m * a - l * b));
                     }
                     if (IMG) {
                         atomicAdd(acc + 3 * g.nd, (double)glam[r % RI][cc]);

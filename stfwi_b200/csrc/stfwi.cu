@@ -60,6 +60,8 @@ struct stfwi_handle {
     int accp = 5;   // accumulator planes per shot group (7 with the density terms)
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
     CUtensorMap tmUo{}, tmSo{}, tmPQo{}, tmEo{};   // own-cell boxes of the two-column kernels
+    CUtensorMap tmH{};        // history [shot][slot*snf + field][nz_dom][nx_dom] (own-cell carry-in boxes)
+    bool hist_tma = false;    // tmH valid: pad and nx_dom multiples of 4 (16-byte box rows)
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
     // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
     // variant 2: 32 x 8*RPT3 and 32 x 32)
@@ -543,7 +545,7 @@ void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, 
     auto launch = [&](auto kern) {
         kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L4<FD>::bytes(L4<FD>::ADB, 2), st>>>(
             h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
-            h->tmPQ, h->tmEo);
+            h->tmPQ, h->tmEo, h->tmH);
     };
     const bool rho = h->g.snf == 5;
     if (ao.want_exact && ao.want_img) rho ? launch(k4_adj_b<FD, true, true, true>) : launch(k4_adj_b<FD, true, true, false>);
@@ -816,6 +818,16 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
         if ((r = encode(h, &h->tmPQo, h->A, 4, fdims, fstr, own2))) return r;
         const cuuint32_t own3b[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->thb, 3, 1};
         if ((r = encode(h, &h->tmEo, h->A, 4, fdims, fstr, own3b))) return r;
+        // the history box starts at column j0 - pad and its rows are nx_dom
+        // floats: both must be multiples of 16 bytes for a tensor copy
+        if (h->snap && h->d.pad % 4 == 0 && g.nx_dom % 4 == 0) {
+            const cuuint64_t hdims[4] = {(cuuint64_t)g.nx_dom, (cuuint64_t)g.nz_dom,
+                                         (cuuint64_t)g.snf * h->slots, S};
+            const cuuint64_t hstr[3] = {(cuuint64_t)g.nx_dom * 4, (cuuint64_t)g.nd * 4,
+                                        (cuuint64_t)h->slots * g.snf * g.nd * 4};
+            if ((r = encode(h, &h->tmH, h->snap, 4, hdims, hstr, own3b))) return r;
+            h->hist_tma = true;
+        }
     }
     return STFWI_OK;
 }
@@ -1275,7 +1287,7 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
             // outputs of step n + 1: the next slot inside a segment, else the
             // extra slot filled from the following segment (checkpoints)
             ao.slot_next = (n + 1 < seg1) ? n - seg0 + 2 : (h->ncp > 0 && n + 1 < g.nt ? h->ck + 1 : -1);
-            ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im;
+            ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im; ao.hist_tma = h->hist_tma ? 1 : 0;
             ao.src_a = sr ? src_dev : nullptr; ao.rec_adj = h->rec_adj; ao.ping = ping;
             switch (h->d.fd_order) {
             case 2: launch_adj_step<2>(h, n, ai, ao, s); break;
@@ -1560,7 +1572,7 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
             AdjOut ao{};
             ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = 0; ao.slot_img = h->slots > 1 ? 1 : -1;
             ao.slot_next = -1; ao.accp = h->accp; ao.acc = h->acc; ao.want_exact = ex; ao.want_img = 0;
-            ao.rec_adj = h->rec_adj; ao.ping = n & 1;
+            ao.rec_adj = h->rec_adj; ao.ping = n & 1; ao.hist_tma = h->hist_tma ? 1 : 0;
             switch (h->d.fd_order) {
             case 2: launch_adj_step<2>(h, n, ai, ao, st); break;
             case 4: launch_adj_step<4>(h, n, ai, ao, st); break;
