@@ -29,6 +29,14 @@ EXPORTS = (
     "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
 )
 
+# every symbol include/stfwi_nn.h declares (the learned preconditioner's network kernels)
+NN_EXPORTS = (
+    "stfwi_nn_last_error", "stfwi_nn_check", "stfwi_nn_conv3x3", "stfwi_nn_conv3x3_dgrad",
+    "stfwi_nn_conv3x3_wgrad", "stfwi_nn_pack_input", "stfwi_nn_avgpool2", "stfwi_nn_skip_grad",
+    "stfwi_nn_upsample2", "stfwi_nn_upsample2_grad", "stfwi_nn_head", "stfwi_nn_head_loss_grad",
+    "stfwi_nn_bias_grad", "stfwi_nn_pack_weights", "stfwi_nn_adam",
+)
+
 PRECOND_ILLUM, PRECOND_EPRECOND3 = 0, 1
 
 NOALLOC_MAX_TRACES = 1 << 18
@@ -97,5 +105,22 @@ def load():
         L.stfwi_preconditioner.argtypes = [H, i32, i32, f64, vp, vp]
         L.stfwi_project_velocity.argtypes = [ct.c_int64, vp, vp, vp, f64, f64, f64, f64, vp]
         L.stfwi_autotune.argtypes = [H, i32, vp, vp]
+        sz, f32 = ct.c_size_t, ct.c_float
+        L.stfwi_nn_last_error.argtypes = []
+        L.stfwi_nn_last_error.restype = ct.c_char_p
+        L.stfwi_nn_check.argtypes = [vp]
+        L.stfwi_nn_conv3x3.argtypes = [vp, i32, i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp]
+        L.stfwi_nn_conv3x3_dgrad.argtypes = [vp, i32, i32, i32, i32, vp, i32, vp, i32, i32, vp, vp]
+        L.stfwi_nn_conv3x3_wgrad.argtypes = [vp, vp, i32, i32, i32, i32, i32, vp, vp]
+        L.stfwi_nn_pack_input.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp, vp]
+        L.stfwi_nn_avgpool2.argtypes = [vp, i32, i32, i32, i32, i32, i32, vp, vp]
+        L.stfwi_nn_skip_grad.argtypes = [vp, vp, i32, i32, vp, i32, i32, i32, i32, vp, vp]
+        L.stfwi_nn_upsample2.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp]
+        L.stfwi_nn_upsample2_grad.argtypes = [vp, i32, vp, i32, i32, i32, i32, vp, vp]
+        L.stfwi_nn_head.argtypes = [vp, sz, i32, vp, vp, vp, vp]
+        L.stfwi_nn_head_loss_grad.argtypes = [vp, sz, i32, vp, vp, vp, vp, f32, vp, vp, vp, vp, vp]
+        L.stfwi_nn_bias_grad.argtypes = [vp, sz, i32, vp, vp]
+        L.stfwi_nn_pack_weights.argtypes = [vp, i32, i32, vp, vp, vp]
+        L.stfwi_nn_adam.argtypes = [vp, vp, vp, vp, sz, f32, f32, f32, f32, f32, vp]
         _lib = L
     return _lib

@@ -6,9 +6,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libstfwi.so")
-SOURCES = [os.path.join(HERE, "csrc", "stfwi.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "kernels_v3.cuh", "kernels_v4.cuh", "tma.cuh", "post.cuh")] \
-    + [os.path.join(ROOT, "include", "stfwi.h")]
+SOURCES = [os.path.join(HERE, "csrc", "stfwi.cu"), os.path.join(HERE, "csrc", "nn.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("kernels.cuh", "kernels_v3.cuh", "kernels_v4.cuh", "tma.cuh", "post.cuh", "umma.cuh")] \
+    + [os.path.join(ROOT, "include", f) for f in ("stfwi.h", "stfwi_nn.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -9,8 +9,8 @@ import pytest
 from tests.conftest import ROOT
 
 
-def _declared():
-    src = open(os.path.join(ROOT, "include", "stfwi.h")).read()
+def _declared(header="stfwi.h"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(stfwi_[a-z_0-9]+)\s*\(", src)))
 
@@ -23,6 +23,35 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) == set(N.EXPORTS), set(names) ^ set(N.EXPORTS)
+
+
+def test_library_exports_every_network_symbol():
+    """include/stfwi_nn.h (the learned preconditioner's kernels)."""
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    names = _declared("stfwi_nn.h")
+    assert len(names) >= 14
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(N.NN_EXPORTS), set(names) ^ set(N.NN_EXPORTS)
+
+
+def test_network_calls_reject_bad_shapes_on_the_host():
+    """Shape checks run before any launch, so they answer without a GPU."""
+    from stfwi_b200 import _native as N
+    lib = N.load()
+    x = ct.c_void_p(16)
+    # channel count not a multiple of 16
+    assert lib.stfwi_nn_conv3x3(x, 1, 128, 128, 24, x, 32, None, 1, x, 32, 0, None) == N.STFWI_ERR_INVALID
+    assert b"multiples of 16" in lib.stfwi_nn_last_error()
+    # 100 pixels wide does not tile into 128-pixel boxes
+    assert lib.stfwi_nn_conv3x3(x, 1, 128, 100, 32, x, 32, None, 1, x, 32, 0, None) == N.STFWI_ERR_INVALID
+    # output slice past the channel stride
+    assert lib.stfwi_nn_conv3x3(x, 1, 128, 128, 32, x, 32, None, 1, x, 48, 24, None) == N.STFWI_ERR_INVALID
+    # weight gradient width not a multiple of 64
+    assert lib.stfwi_nn_conv3x3_wgrad(x, x, 1, 64, 96, 32, 32, x, None) == N.STFWI_ERR_INVALID
+    # unaligned pointer
+    assert lib.stfwi_nn_conv3x3(ct.c_void_p(8), 1, 128, 128, 32, x, 32, None, 1, x, 32, 0, None) == N.STFWI_ERR_INVALID
 
 
 def test_workspace_and_grid_shape_are_host_only():
