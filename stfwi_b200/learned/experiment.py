@@ -1,0 +1,277 @@
+"""Training data, training and evaluation of the learned preconditioner.
+
+* pairs: for each seeded layered-fault model, the plain method (lockstep
+  L-BFGS, ``inversion.lbfgs``) runs ``n_iter`` iterations from the smoothed
+  start; the input is [preconditioned first gradient, illumination
+  preconditioner, Vp, Vs] at the start and the target is the Vs update
+  the iterations made.
+* training: Adam on the masked mean-square error of the U-Net
+  (``unet.UNet``, tcgen05 kernels), left-right mirror images as
+  augmentation.
+* evaluation on held-out models: the plain method for ``n_plain``
+  iterations sets each model's target Vs error (the lowest relative RMS
+  error it reached); the learned method evaluates the gradient at the
+  start, takes the network's direction with a misfit line search (the step
+  is accepted only if it lowers the misfit, otherwise the model falls back
+  to the plain method from the start) and continues with plain L-BFGS until
+  it reaches the same error.  Reported: wall time to the target for both.
+
+``python -m stfwi_b200.learned.experiment --train 192 --test 16 --out DIR``
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import time
+
+import numpy as np
+
+from . import inversion as I
+from .unet import UNet, padded_shape
+
+TARGET_SCALE = 100.0      # m/s per unit of the network's output
+
+
+def features(g_raw, precond, vp, vs):
+    """[4, nz, nx] FP32 network input: the preconditioned gradient over its
+    largest magnitude, the preconditioner (in [0, 1]), (Vp - 3000) / 1000 and
+    (Vs - 1700) / 500."""
+    g = np.asarray(g_raw, np.float64) * np.asarray(precond, np.float64)
+    g = g / max(float(np.abs(g).max()), 1e-300)
+    return np.stack([g, np.asarray(precond, np.float64), (np.asarray(vp, np.float64) - 3000.0) / 1000.0,
+                     (np.asarray(vs, np.float64) - 1700.0) / 500.0]).astype(np.float32)
+
+
+def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
+    """Training pairs of the given model seeds: (inputs [n, 4, nz, nx],
+    targets [n, nz, nx] in units of TARGET_SCALE, seconds spent)."""
+    X, Y = [], []
+    t0 = time.perf_counter()
+    batch = I.ModelBatch(K, geom)
+    try:
+        for g0 in range(0, len(seeds), K):
+            group = list(seeds[g0:g0 + K])
+            models = [I.true_and_initial(s, geom) for s in group]
+            first = {}
+            gens = []
+            for k in range(K):
+                if k >= len(group):
+                    gens.append(None)
+                    continue
+                batch.load(k, *models[k])
+
+                def rec(x, f, graw, k=k):
+                    first.setdefault(k, graw.copy())
+                gens.append(I.lbfgs(models[k][1][0], models[k][1][1], batch.precond[k], n_iter, record=rec))
+            finals, _ = I.run_lockstep(batch, gens)
+            for k in range(len(group)):
+                init = models[k][1]
+                X.append(features(first[k], batch.precond[k], init[1], init[0]))
+                Y.append(((finals[k] - init[0]) / TARGET_SCALE).astype(np.float32))
+            log(f"pairs {len(X)}/{len(seeds)}  {time.perf_counter() - t0:.1f} s")
+    finally:
+        batch.close()
+    return np.stack(X), np.stack(Y), time.perf_counter() - t0
+
+
+def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
+    """Adam with a cosine learning-rate decay on the pairs (and their
+    mirror images); the last ``n_val`` pairs are held out as validation.
+    Returns (network, per-epoch (train loss, validation loss))."""
+    import torch
+    n_all, _, nz, nx = X.shape
+    n = n_all - n_val
+    h, w = padded_shape(nz, nx)
+    net = UNet(h, w, seed=seed)
+    Xd = torch.from_numpy(np.ascontiguousarray(X[:n])).cuda()
+    Yd = torch.from_numpy(np.ascontiguousarray(Y[:n])).cuda()
+    tgt = torch.zeros((batch, h, w), device="cuda")
+    wgt = torch.zeros((batch, h, w), device="cuda")
+    wgt[:, :nz, :nx] = 1.0
+    inv = 1.0 / (batch * nz * nx)
+    rng = np.random.default_rng(seed)
+    per_epoch = (2 * n) // batch
+    total = max(epochs * per_epoch, 1)
+    hist = []
+    step = 0
+    for ep in range(epochs):
+        perm = rng.permutation(2 * n)
+        acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+        for b0 in range(0, per_epoch * batch, batch):
+            idx = torch.from_numpy(perm[b0:b0 + batch]).cuda()
+            src, flip = idx % n, (idx >= n)
+            xb, yb = Xd[src], Yd[src]
+            xb = torch.where(flip[:, None, None, None], xb.flip(-1), xb)
+            yb = torch.where(flip[:, None, None], yb.flip(-1), yb)
+            tgt[:, :nz, :nx] = yb
+            lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * step / total))
+            acc += net.train_step(net.pack(xb), tgt, wgt, lr_t, inv_norm=inv)
+            step += 1
+        tr = float(acc) / max(per_epoch, 1)
+        va = validation_loss(net, X[n:], Y[n:], batch) if n_val else float("nan")
+        hist.append((tr, va))
+        log(f"epoch {ep + 1}/{epochs}  train {tr:.5f}  val {va:.5f}")
+    net.check()
+    return net, hist
+
+
+def predict(net, X, batch=8):
+    """Network output on inputs [n, 4, nz, nx] -> [n, nz, nx] (units of TARGET_SCALE)."""
+    import torch
+    n, _, nz, nx = X.shape
+    out = []
+    for b0 in range(0, n, batch):
+        xb = torch.from_numpy(np.ascontiguousarray(X[b0:b0 + batch])).cuda()
+        o = net.forward(net.pack(xb))
+        out.append(o[:, :nz, :nx].cpu().numpy())
+    return np.concatenate(out)
+
+
+def validation_loss(net, X, Y, batch=8):
+    """Mean-square error of the prediction over the validation pairs, and
+    that of predicting zero (the target's mean square) for scale."""
+    P = predict(net, X, batch)
+    return float(np.mean((P.astype(np.float64) - Y) ** 2))
+
+
+def _first_time(hist, target):
+    """Clock time of the first recorded iterate whose Vs error is <= target."""
+    for t, err, _f in hist:
+        if err <= target * (1.0 + 1e-12):
+            return t
+    return None
+
+
+def evaluate(net, seeds, K=4, n_plain=20, geom=I.GEOMETRY, alphas=(1.0, 0.5, 0.25), log=print):
+    """Learned vs plain on held-out models; one record per model."""
+    import torch
+    out = []
+    batch = I.ModelBatch(K, geom)
+    try:
+        for g0 in range(0, len(seeds), K):
+            group = list(seeds[g0:g0 + K])
+            models = [I.true_and_initial(s, geom) for s in group]
+            slots = list(range(len(group)))
+            for k in slots:
+                batch.load(k, *models[k])
+            true_vs = {k: models[k][0][0] for k in slots}
+            vs0 = {k: models[k][1][0].astype(np.float64) for k in slots}
+            vp0 = {k: models[k][1][1] for k in slots}
+            # plain: n_plain iterations set the target error of every model
+            clock = {"t": 0.0}
+            plain = {k: [] for k in slots}
+            gens = [I.lbfgs(vs0[k], vp0[k], batch.precond[k], n_plain,
+                            record=lambda x, f, g, k=k: plain[k].append((clock["t"], I.vs_rel_rms(x, true_vs[k]), f)))
+                    for k in slots] + [None] * (K - len(group))
+            I.run_lockstep(batch, gens, clock)
+            target = {k: min(e for _, e, _ in plain[k]) for k in slots}
+            # learned: gradient at the start, the network's direction, a misfit line search
+            clock = {"t": 0.0}
+            learned = {k: [] for k in slots}
+            t0 = time.perf_counter()
+            res = batch.evaluate([vs0[k] if k in slots else None for k in range(K)])
+            clock["t"] += time.perf_counter() - t0
+            f0 = {k: res[k][0] for k in slots}
+            for k in slots:
+                learned[k].append((clock["t"], I.vs_rel_rms(vs0[k], true_vs[k]), f0[k]))
+            t0 = time.perf_counter()
+            X = np.stack([features(res[k][1], batch.precond[k], vp0[k], vs0[k]) for k in slots])
+            d = predict(net, X) * TARGET_SCALE
+            torch.cuda.synchronize()
+            t_net = time.perf_counter() - t0
+            clock["t"] += t_net
+            accepted, step = {}, {}
+            for a in alphas:
+                cand = [None] * K
+                for k in slots:
+                    if k not in accepted:
+                        cand[k] = I.project_vs(vs0[k] + a * d[k], vp0[k])
+                if all(c is None for c in cand):
+                    break
+                t0 = time.perf_counter()
+                fs = batch.misfits(cand)
+                clock["t"] += time.perf_counter() - t0
+                for k in slots:
+                    if cand[k] is not None and fs[k] < f0[k]:
+                        accepted[k], step[k] = cand[k], a
+                        learned[k].append((clock["t"], I.vs_rel_rms(cand[k], true_vs[k]), fs[k]))
+            gens = []
+            for k in range(K):
+                if k not in slots:
+                    gens.append(None)
+                    continue
+                x1 = accepted.get(k, vs0[k])            # rejected: the plain method from the start
+                gens.append(I.lbfgs(x1, vp0[k], batch.precond[k], n_plain,
+                                    record=lambda x, f, g, k=k: learned[k].append(
+                                        (clock["t"], I.vs_rel_rms(x, true_vs[k]), f)),
+                                    stop=lambda x, f, k=k: I.vs_rel_rms(x, true_vs[k]) <= target[k]))
+            I.run_lockstep(batch, gens, clock)
+            for k in slots:
+                tp = _first_time(plain[k], target[k])
+                tl = _first_time(learned[k], target[k])
+                rec = dict(seed=int(group[k]), err_start=plain[k][0][1], target=target[k],
+                           plain_time_s=tp, learned_time_s=tl,
+                           ratio=(tl / tp) if (tl is not None and tp) else None,
+                           learned_step_accepted=k in accepted, step=step.get(k),
+                           err_after_learned_step=I.vs_rel_rms(accepted[k], true_vs[k]) if k in accepted else None,
+                           err_plain_final=plain[k][-1][1], err_learned_final=learned[k][-1][1],
+                           plain_iterates=len(plain[k]), learned_iterates=len(learned[k]),
+                           network_s=t_net / len(group))
+                out.append(rec)
+                log(json.dumps(rec))
+    finally:
+        batch.close()
+    return out
+
+
+def summarize(records):
+    ratios = [r["ratio"] for r in records if r["ratio"] is not None]
+    after = [r["err_after_learned_step"] for r in records if r["err_after_learned_step"] is not None]
+    return dict(models=len(records), reached_target=sum(r["learned_time_s"] is not None for r in records),
+                learned_step_accepted=sum(bool(r["learned_step_accepted"]) for r in records),
+                median_time_ratio=float(np.median(ratios)) if ratios else None,
+                mean_time_ratio=float(np.mean(ratios)) if ratios else None,
+                median_err_start=float(np.median([r["err_start"] for r in records])),
+                median_target=float(np.median([r["target"] for r in records])),
+                median_err_after_learned_step=float(np.median(after)) if after else None)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="learned preconditioner: data, training, evaluation")
+    ap.add_argument("--train", type=int, default=192, help="training models (seeds 1000, 1001, ...)")
+    ap.add_argument("--test", type=int, default=16, help="held-out models (seeds 5000, 5001, ...)")
+    ap.add_argument("--iters", type=int, default=10, help="L-BFGS iterations of a training pair")
+    ap.add_argument("--plain", type=int, default=20, help="L-BFGS iterations of the plain arm")
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--val", type=int, default=16, help="training pairs held out for validation")
+    ap.add_argument("--K", type=int, default=4, help="models evaluated concurrently")
+    ap.add_argument("--out", default="learned_out")
+    a = ap.parse_args(argv)
+    os.makedirs(a.out, exist_ok=True)
+    logf = open(os.path.join(a.out, "log.txt"), "a")
+
+    def log(msg):
+        print(msg, flush=True)
+        logf.write(msg + "\n")
+        logf.flush()
+
+    X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log)
+    n_val = min(a.val, X.shape[0] // 4)
+    t0 = time.perf_counter()
+    net, hist = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
+    t_train = time.perf_counter() - t0
+    zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
+    np.savez_compressed(os.path.join(a.out, "unet_weights.npz"), **net.state_dict())
+    recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
+    summary = dict(config=dict(vars(a), geometry=I.GEOMETRY), data_seconds=t_data, train_seconds=t_train,
+                   train_history=hist, val_loss_of_zero_prediction=zero_val,
+                   evaluation=summarize(recs), records=recs)
+    with open(os.path.join(a.out, "results.json"), "w") as fh:
+        json.dump(summary, fh, indent=1)
+    log(json.dumps(summary["evaluation"]))
+
+
+if __name__ == "__main__":
+    main()
