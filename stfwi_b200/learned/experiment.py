@@ -130,8 +130,7 @@ def predict(net, X, batch=8):
 
 
 def validation_loss(net, X, Y, batch=8):
-    """Mean-square error of the prediction over the validation pairs, and
-    that of predicting zero (the target's mean square) for scale."""
+    """Mean-square error of the prediction over the validation pairs."""
     P = predict(net, X, batch)
     return float(np.mean((P.astype(np.float64) - Y) ** 2))
 

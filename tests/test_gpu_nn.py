@@ -178,10 +178,16 @@ def _network_case(B=2, seed=0):
     return net, feat, x, tgt, wgt
 
 
+_FORWARD = ("a1", "cat1", "p1", "a2", "cat2", "p2", "a3", "cat3", "p3", "b1", "b2", "d3a", "d3b", "d2a", "d2b",
+            "d1a", "d1b", "out")
+
+
 def _emulated(net_gpu, x, tgt, wgt, inv, monkeypatch):
     """The same network run by the same host code on the CPU with every
     kernel replaced by its torch restatement (tests/fake_nn.py) storing BF16
-    at the same points as the kernels: (output, loss, gradients)."""
+    at the same points as the kernels.  Returns its forward output, then the
+    loss and gradients of its backward pass run on the GPU's own forward
+    activations, so that both backward passes see the same ReLU masks."""
     from stfwi_b200 import _native as N
     from stfwi_b200.learned import unet as U
     from tests.fake_nn import FakeNN
@@ -193,18 +199,23 @@ def _emulated(net_gpu, x, tgt, wgt, inv, monkeypatch):
         net.pack_weights()
         xc = x.cpu()
         out = net.forward(xc, train=True).clone()
+        b, bg = net.buffers(x.shape[0], True), net_gpu.buffers(x.shape[0], True)
+        for k in _FORWARD:
+            b[k].copy_(bg[k].cpu())
         loss = net.backward(xc, tgt.cpu(), wgt.cpu(), inv)
         return out, float(loss), net.grads.clone()
 
 
 def test_unet_forward_and_gradients_match_torch(monkeypatch):
     """The whole network (14 tensor-core convolutions, pooling, upsampling,
-    concatenation, head, masked MSE): (1) against the torch restatement of
-    every op with the same BF16 storage points, to FP32-accumulation
-    tolerance (rel-L2 <= 1e-2 on the output and every parameter gradient);
-    (2) against the FP32 torch U-Net with the same weights, where the BF16
-    rounding of activations and gradients (and the ReLU masks it flips)
-    leaves 1-2 % on the output and up to ~12 % on the deepest gradients."""
+    concatenation, head, masked MSE).  (1) Against the torch restatement of
+    every op with the same BF16 storage points: forward output rel-L2 <=
+    1e-2; backward pass on the same forward activations, every parameter
+    gradient rel-L2 <= 1e-2.  (2) Against the FP32 torch U-Net with the same
+    weights: output <= 3e-2; the gradients only within 0.2, because a loss
+    with random targets makes each gradient a sum of many random-sign terms,
+    so the few ReLU masks that BF16 activations flip move it by about
+    sqrt(flipped fraction) (observed 2-12 %)."""
     import torch
     from stfwi_b200.learned.unet import LAYERS, param_layout
     from tests.unet_ref import masked_mse, unet_forward
@@ -229,7 +240,7 @@ def test_unet_forward_and_gradients_match_torch(monkeypatch):
     emu = per_block(grads, e_grad)
     print("vs BF16-storage emulation: out", _rel(out, e_out), {k: (round(a, 5), round(b, 5)) for k, (a, b) in emu.items()})
     assert _rel(out, e_out) < 1e-2
-    assert abs(loss / e_loss - 1) < 1e-2
+    assert abs(loss / e_loss - 1) < 1e-4
     assert max(max(v) for v in emu.values()) < 1e-2, emu
 
     params = net.params.detach().double().cpu().requires_grad_(True)
