@@ -64,11 +64,11 @@ def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
 
                 def rec(x, f, graw, k=k):
                     first.setdefault(k, graw.copy())
-                gens.append(I.lbfgs(models[k][1][0], models[k][1][1], batch.precond[k], n_iter, record=rec))
+                gens.append(I.lbfgs(models[k][1][0], batch.vp[k], batch.precond[k], n_iter, record=rec))
             finals, _ = I.run_lockstep(batch, gens)
             for k in range(len(group)):
                 init = models[k][1]
-                X.append(features(first[k], batch.precond[k], init[1], init[0]))
+                X.append(features(first[k], batch.precond[k], batch.vp[k], init[0]))
                 Y.append(((finals[k] - init[0]) / TARGET_SCALE).astype(np.float32))
             log(f"pairs {len(X)}/{len(seeds)}  {time.perf_counter() - t0:.1f} s")
     finally:
@@ -78,8 +78,9 @@ def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
 
 def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
     """Adam with a cosine learning-rate decay on the pairs (and their
-    mirror images); the last ``n_val`` pairs are held out as validation.
-    Returns (network, per-epoch (train loss, validation loss))."""
+    mirror images); the last ``n_val`` pairs are held out as validation and
+    the weights of the epoch with the lowest validation loss are kept.
+    Returns (network, per-epoch (train loss, validation loss), best epoch)."""
     import torch
     n_all, _, nz, nx = X.shape
     n = n_all - n_val
@@ -96,6 +97,7 @@ def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
     total = max(epochs * per_epoch, 1)
     hist = []
     step = 0
+    best = (float("inf"), -1, None)
     for ep in range(epochs):
         perm = rng.permutation(2 * n)
         acc = torch.zeros(1, dtype=torch.float64, device="cuda")
@@ -113,8 +115,13 @@ def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
         va = validation_loss(net, X[n:], Y[n:], batch) if n_val else float("nan")
         hist.append((tr, va))
         log(f"epoch {ep + 1}/{epochs}  train {tr:.5f}  val {va:.5f}")
+        if n_val and va < best[0]:
+            best = (va, ep, net.params.detach().clone())
+    if best[2] is not None:
+        net.params.copy_(best[2])
+        net.pack_weights()
     net.check()
-    return net, hist
+    return net, hist, best[1] + 1
 
 
 def predict(net, X, batch=8):
@@ -157,7 +164,7 @@ def evaluate(net, seeds, K=4, n_plain=20, geom=I.GEOMETRY, alphas=(1.0, 0.5, 0.2
                 batch.load(k, *models[k])
             true_vs = {k: models[k][0][0] for k in slots}
             vs0 = {k: models[k][1][0].astype(np.float64) for k in slots}
-            vp0 = {k: models[k][1][1] for k in slots}
+            vp0 = {k: batch.vp[k] for k in slots}          # the known background
             # plain: n_plain iterations set the target error of every model
             clock = {"t": 0.0}
             plain = {k: [] for k in slots}
@@ -243,7 +250,7 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=16, help="held-out models (seeds 5000, 5001, ...)")
     ap.add_argument("--iters", type=int, default=10, help="L-BFGS iterations of a training pair")
     ap.add_argument("--plain", type=int, default=20, help="L-BFGS iterations of the plain arm")
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--val", type=int, default=16, help="training pairs held out for validation")
     ap.add_argument("--K", type=int, default=4, help="models evaluated concurrently")
     ap.add_argument("--out", default="learned_out")
@@ -259,13 +266,13 @@ def main(argv=None):
     X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log)
     n_val = min(a.val, X.shape[0] // 4)
     t0 = time.perf_counter()
-    net, hist = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
+    net, hist, best_epoch = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
     t_train = time.perf_counter() - t0
     zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
     np.savez_compressed(os.path.join(a.out, "unet_weights.npz"), **net.state_dict())
     recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
     summary = dict(config=dict(vars(a), geometry=I.GEOMETRY), data_seconds=t_data, train_seconds=t_train,
-                   train_history=hist, val_loss_of_zero_prediction=zero_val,
+                   train_history=hist, best_epoch=best_epoch, val_loss_of_zero_prediction=zero_val,
                    evaluation=summarize(recs), records=recs)
     with open(os.path.join(a.out, "results.json"), "w") as fh:
         json.dump(summary, fh, indent=1)

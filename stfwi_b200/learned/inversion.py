@@ -55,7 +55,7 @@ def vs_rel_rms(vs, vs_true):
     return float(np.sqrt(np.mean((vs - t) ** 2)) / np.sqrt(np.mean(t ** 2)))
 
 
-def project_vs(vs, vp, vs_min=300.0, ratio=1.25):
+def project_vs(vs, vp, vs_min=300.0, ratio=1.2):
     """Vs bounds of the inversion: vs_min <= Vs <= Vp / ratio (Vp fixed)."""
     return np.clip(vs, vs_min, np.asarray(vp, np.float64) / ratio)
 
@@ -157,8 +157,10 @@ def run_lockstep(batch, gens, clock=None):
 class ModelBatch:
     """K solver handles (one per model slot) on K CUDA streams, same
     acquisition.  ``load(k, true, init)`` models the observed data of slot
-    k from its true model, fixes its Vp and rho at the initial model's and
-    computes the illumination preconditioner there; ``evaluate`` runs one
+    k from its true model, fixes its Vp and rho (the true ones: the
+    experiments invert Vs with a known P-velocity and density background,
+    so that the Vs error measures the Vs update alone) and computes the
+    illumination preconditioner at the initial Vs; ``evaluate`` runs one
     round of misfit + exact gradient evaluations."""
 
     def __init__(self, K, geom=GEOMETRY, mem_budget_gb=28.0):
@@ -190,9 +192,11 @@ class ModelBatch:
         self.precond = [None] * self.K
         self.evals = 0
 
-    def load(self, k, true, init):
+    def load(self, k, true, init, known_background=True):
         """Observed data of slot k (component ``geom['component']``) from the
-        true model; background Vp, rho and the preconditioner from ``init``."""
+        true model; the background Vp and rho are the true ones (or the
+        initial ones with ``known_background=False``); the preconditioner
+        comes from the initial Vs on that background."""
         torch = self.torch
         S, st = self.solvers[k], self.streams[k]
         comp = self.geom["component"]
@@ -203,9 +207,10 @@ class ModelBatch:
             S.records(out=rec)
             self.obs[k].copy_(rec[:, comp])
             self.scale[k] = float(1.0 / (float(self.obs[k].double().pow(2).mean()) + 1e-45))
-            self.vp[k] = np.asarray(init[1], np.float64)
-            self.rho[k] = np.asarray(init[2], np.float64)
-            S.set_model(*init)
+            bg = true if known_background else init
+            self.vp[k] = np.asarray(bg[1], np.float64)
+            self.rho[k] = np.asarray(bg[2], np.float64)
+            S.set_model(init[0], bg[1], bg[2])
             self.precond[k] = S.preconditioner("illum", comp, 1e-3)
         st.synchronize()
 
