@@ -152,38 +152,53 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     const uint32_t layout = umma_layout_for((int)aw);
     const uint32_t sbase = smem_u32(base);
 
-    if (threadIdx.x == 0) {
+    // warp 0 streams the operand boxes and warp 1 issues the MMAs; a whole warp runs
+    // each loop (lane 0 waits and issues, the other lanes wait at the shuffle), so
+    // no lane of a working warp spins on the accumulator barrier meanwhile
+    const int lane = threadIdx.x & 31;
+    if (warp == 0) {
         // producer: one A box (128 shifted pixels x kc channels) and one B box (bn x kc weights) per k-block
         for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % STAGES;
-            if (kb >= STAGES && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, NN_WAIT)) {
-                atomicExch(err, 1);
-                break;
+            int fail = 0;
+            if (lane == 0) {
+                const int s = kb % STAGES;
+                if (kb >= STAGES && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, NN_WAIT)) {
+                    atomicExch(err, 1);
+                    fail = 1;
+                } else {
+                    const int tap = kb / nkc, c0 = (kb % nkc) * g.kc;
+                    mbar_arrive_expect_tx(&full[s], a_bytes + b_bytes);
+                    tma_load_4d(base + s * st_bytes, &tmX, &full[s], c0, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img);
+                    tma_load_3d(base + s * st_bytes + a_bytes, &tmW, &full[s], c0, n0, tap);
+                }
             }
-            const int tap = kb / nkc, c0 = (kb % nkc) * g.kc;
-            mbar_arrive_expect_tx(&full[s], a_bytes + b_bytes);
-            tma_load_4d(base + s * st_bytes, &tmX, &full[s], c0, w0 + tap % 3 - 1, h0 + tap / 3 - 1, img);
-            tma_load_3d(base + s * st_bytes + a_bytes, &tmW, &full[s], c0, n0, tap);
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
         }
-    } else if (threadIdx.x == 32) {
+    } else if (warp == 1) {
         // MMA issuer: kc/16 MMAs (K = 16) per k-block, the K step is +32 bytes inside the swizzle atom
         const uint32_t idesc = umma_idesc_bf16(128, g.bn, 0, 0);
         for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % STAGES;
-            if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, NN_WAIT)) {
-                atomicExch(err, 2);
-                break;
+            int fail = 0;
+            if (lane == 0) {
+                const int s = kb % STAGES;
+                if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, NN_WAIT)) {
+                    atomicExch(err, 2);
+                    fail = 1;
+                } else {
+                    tmem_fence_after();
+                    const uint32_t sa = sbase + s * st_bytes, sb = sa + a_bytes;
+                    for (int k = 0; k < g.kc / 16; ++k) {
+                        const uint64_t ad = umma_smem_desc(sa + 32u * k, 16u, 8u * aw, layout);
+                        const uint64_t bd = umma_smem_desc(sb + 32u * k, 16u, 8u * aw, layout);
+                        umma_bf16(tmem, ad, bd, idesc, (kb | k) != 0);
+                    }
+                    umma_commit(&empty[s]);
+                }
             }
-            tmem_fence_after();
-            const uint32_t sa = sbase + s * st_bytes, sb = sa + a_bytes;
-            for (int k = 0; k < g.kc / 16; ++k) {
-                const uint64_t ad = umma_smem_desc(sa + 32u * k, 16u, 8u * aw, layout);
-                const uint64_t bd = umma_smem_desc(sb + 32u * k, 16u, 8u * aw, layout);
-                umma_bf16(tmem, ad, bd, idesc, (kb | k) != 0);
-            }
-            umma_commit(&empty[s]);
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
         }
-        umma_commit(done);
+        if (lane == 0) umma_commit(done);
+        __syncwarp();
     }
 
     // epilogue: thread m owns accumulator row m (TMEM lane m) = pixel m of the box
@@ -273,45 +288,58 @@ __global__ void __launch_bounds__(CONV_THREADS, 1)
     const int wchunks = g.w / WG_PIX;
     const int dy = tap / 3 - 1, dx = tap % 3 - 1;
 
-    if (threadIdx.x == 0 && nk > 0) {
+    const int lane = threadIdx.x & 31;
+    if (warp == 0 && nk > 0) {
         for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % STAGES;
-            if (kb >= STAGES && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, NN_WAIT)) {
-                atomicExch(err, 11);
-                break;
+            int fail = 0;
+            if (lane == 0) {
+                const int s = kb % STAGES;
+                if (kb >= STAGES && !mbar_wait_bounded(&empty[s], ((kb / STAGES) - 1) & 1, NN_WAIT)) {
+                    atomicExch(err, 11);
+                    fail = 1;
+                } else {
+                    int c = c_begin + kb;
+                    const int px0 = (c % wchunks) * WG_PIX;
+                    c /= wchunks;
+                    const int hh = c % g.h, img = c / g.h;
+                    mbar_arrive_expect_tx(&full[s], na_live * col_a + b_bytes);
+                    uint8_t *sa = base + s * st_bytes;
+                    for (int a = 0; a < na_live; ++a)
+                        tma_load_4d(sa + a * col_a, &tmDZ, &full[s], m0 + a * g.ae_a, px0, hh, img);
+                    for (int b = 0; b < nb; ++b)
+                        tma_load_4d(sa + a_bytes + b * col_b, &tmX, &full[s], n0 + b * g.ae_b, px0 + dx, hh + dy,
+                                    img);
+                }
             }
-            int c = c_begin + kb;
-            const int px0 = (c % wchunks) * WG_PIX;
-            c /= wchunks;
-            const int hh = c % g.h, img = c / g.h;
-            mbar_arrive_expect_tx(&full[s], na_live * col_a + b_bytes);
-            uint8_t *sa = base + s * st_bytes;
-            for (int a = 0; a < na_live; ++a)
-                tma_load_4d(sa + a * col_a, &tmDZ, &full[s], m0 + a * g.ae_a, px0, hh, img);
-            for (int b = 0; b < nb; ++b)
-                tma_load_4d(sa + a_bytes + b * col_b, &tmX, &full[s], n0 + b * g.ae_b, px0 + dx, hh + dy, img);
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
         }
-    } else if (threadIdx.x == 32 && nk > 0) {
+    } else if (warp == 1 && nk > 0) {
         // K = 16 pixel rows per MMA: +16 rows of the atom column; LBO = atom column stride, SBO = 8 rows
         const uint32_t idesc = umma_idesc_bf16(128, g.bn, 1, 1);
         const uint32_t la = umma_layout_for((int)aw_a), lb = umma_layout_for((int)aw_b);
         for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % STAGES;
-            if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, NN_WAIT)) {
-                atomicExch(err, 12);
-                break;
-            }
-            tmem_fence_after();
-            const uint32_t sa = sbase + s * st_bytes, sb = sa + a_bytes;
+            int fail = 0;
+            if (lane == 0) {
+                const int s = kb % STAGES;
+                if (!mbar_wait_bounded(&full[s], (kb / STAGES) & 1, NN_WAIT)) {
+                    atomicExch(err, 12);
+                    fail = 1;
+                } else {
+                    tmem_fence_after();
+                    const uint32_t sa = sbase + s * st_bytes, sb = sa + a_bytes;
 #pragma unroll
-            for (int k = 0; k < WG_PIX / 16; ++k) {
-                const uint64_t ad = umma_smem_desc(sa + 16u * aw_a * k, col_a, 8u * aw_a, la);
-                const uint64_t bd = umma_smem_desc(sb + 16u * aw_b * k, col_b, 8u * aw_b, lb);
-                umma_bf16(tmem, ad, bd, idesc, (kb | k) != 0);
+                    for (int k = 0; k < WG_PIX / 16; ++k) {
+                        const uint64_t ad = umma_smem_desc(sa + 16u * aw_a * k, col_a, 8u * aw_a, la);
+                        const uint64_t bd = umma_smem_desc(sb + 16u * aw_b * k, col_b, 8u * aw_b, lb);
+                        umma_bf16(tmem, ad, bd, idesc, (kb | k) != 0);
+                    }
+                    umma_commit(&empty[s]);
+                }
             }
-            umma_commit(&empty[s]);
+            if (__shfl_sync(0xffffffffu, fail, 0)) break;
         }
-        umma_commit(done);
+        if (lane == 0) umma_commit(done);
+        __syncwarp();
     }
 
     if (nk > 0) {
