@@ -27,9 +27,11 @@ from .. import models as Mo
 # acquisition of the learned-preconditioner experiments: the 152 x 500 grid at
 # 20 m (fd8, 20-cell C-PML, free surface), 2000 steps of 1.5 ms, a 5 Hz Ricker,
 # 10 shots every 1000 m alternating vertical force and moment source at 40 m
-# depth, 250 receivers at 20 m depth every 40 m recording vz
+# depth, 250 receivers at 20 m depth every 40 m recording vz; the misfit
+# compares traces low-passed by an order-6 Butterworth filter at `cutoff` Hz
+# (the first band of the reference's multiscale inversion; None: unfiltered)
 GEOMETRY = dict(nz=152, nx=500, dx=20.0, dz=20.0, dt=1.5e-3, nt=2000, fc=5.0, pad=20, fd_order=8,
-                free_surface=True, n_shots=10, component=1)
+                free_surface=True, n_shots=10, component=1, cutoff=3.0)
 
 
 def acquisition(geom=GEOMETRY):
@@ -191,6 +193,10 @@ class ModelBatch:
         self.rho = [None] * self.K
         self.precond = [None] * self.K
         self.evals = 0
+        self.sos = None
+        if g.get("cutoff"):
+            from scipy.signal import butter
+            self.sos = butter(6, g["cutoff"], fs=1.0 / g["dt"], output="sos")
 
     def load(self, k, true, init, known_background=True):
         """Observed data of slot k (component ``geom['component']``) from the
@@ -219,7 +225,7 @@ class ModelBatch:
         S.set_model(np.asarray(vs, np.float32), self.vp[k].astype(np.float32), self.rho[k].astype(np.float32))
         S.forward(store=gradient)
         self.mis[k].zero_()
-        S.misfit(self.obs[k], self.geom["component"], self.scale[k], out=self.mis[k], sync=False)
+        S.misfit(self.obs[k], self.geom["component"], self.scale[k], sos=self.sos, out=self.mis[k], sync=False)
         if gradient:
             self.grad[k].zero_()
             S.gradient(exact=True, out=self.grad[k], sync=False)
