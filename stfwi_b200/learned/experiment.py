@@ -29,7 +29,7 @@ import time
 import numpy as np
 
 from . import inversion as I
-from .unet import UNet, padded_shape
+from .unet import UNet, padded_shape, save_weights
 
 TARGET_SCALE = 100.0      # m/s per unit of the network's output
 
@@ -269,7 +269,7 @@ def main(argv=None):
     net, hist, best_epoch = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
     t_train = time.perf_counter() - t0
     zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
-    np.savez_compressed(os.path.join(a.out, "unet_weights.npz"), **net.state_dict())
+    save_weights(os.path.join(a.out, "unet_weights.npz"), net.params.detach().cpu().numpy())
     recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
     summary = dict(config=dict(vars(a), geometry=I.GEOMETRY), data_seconds=t_data, train_seconds=t_train,
                    train_history=hist, best_epoch=best_epoch, val_loss_of_zero_prediction=zero_val,

@@ -346,3 +346,36 @@ class UNet:
     def check(self):
         """Synchronise and report a tensor-core pipeline wait that gave up."""
         _check(N.load().stfwi_nn_check(self._stream()), "network kernels")
+
+
+def save_weights(path, params):
+    """Store trained parameters compactly: the 3x3 convolution weights as the
+    BF16 values the kernels read (their bits as uint16), the biases and the
+    head in FP32.  Loading gives the network the kernels ran, unchanged."""
+    import torch
+    p = torch.as_tensor(np.asarray(params, dtype=np.float32))
+    lay, head, total = param_layout()
+    if p.numel() != total:
+        raise ValueError("parameter count does not match the network")
+    mask = np.zeros(total, dtype=bool)
+    for wo, bo in lay.values():
+        mask[wo:bo] = True
+    w = p[torch.from_numpy(mask)].to(torch.bfloat16).view(torch.int16).numpy().view(np.uint16)
+    np.savez_compressed(path, conv_bf16=w, rest_f32=p.numpy()[~mask], total=total)
+
+
+def load_weights(path):
+    """FP32 parameter vector from ``save_weights``."""
+    import torch
+    d = np.load(path)
+    lay, _, total = param_layout()
+    if int(d["total"]) != total:
+        raise ValueError(f"{path}: parameter count does not match the network")
+    mask = np.zeros(total, dtype=bool)
+    for wo, bo in lay.values():
+        mask[wo:bo] = True
+    out = np.empty(total, dtype=np.float32)
+    bits = torch.from_numpy(d["conv_bf16"].view(np.int16).copy())
+    out[mask] = bits.view(torch.bfloat16).float().numpy()
+    out[~mask] = d["rest_f32"]
+    return out

@@ -91,3 +91,23 @@ def test_adam_step_matches_the_efficient_form(fake_net):
     w, _ = net.weight("dec2a")
     assert torch.equal(net.wf["dec2a"], w.double())
     assert torch.equal(net.wt["dec2a"], w.double().flip(0).transpose(1, 2))
+
+
+def test_compact_weights_keep_what_the_kernels_read(tmp_path):
+    """The stored network: convolution weights as their BF16 values, biases
+    and head exact; the shipped file loads into a full parameter vector."""
+    import os
+    import torch
+    from stfwi_b200.learned.unet import load_weights, param_layout, save_weights
+    lay, head, total = param_layout()
+    rng = np.random.default_rng(3)
+    p = rng.standard_normal(total).astype(np.float32)
+    save_weights(tmp_path / "w.npz", p)
+    q = load_weights(tmp_path / "w.npz")
+    wo, bo = lay["dec2a"]
+    assert np.array_equal(q[wo:bo], torch.from_numpy(p[wo:bo]).to(torch.bfloat16).float().numpy())
+    assert np.array_equal(q[bo:bo + 64], p[bo:bo + 64])
+    assert np.array_equal(q[head[0]:head[1] + 1], p[head[0]:head[1] + 1])
+    shipped = os.path.join(os.path.dirname(__file__), "..", "stfwi_b200", "learned", "weights", "unet_152x500_3hz.npz")
+    w = load_weights(shipped)
+    assert w.shape == (total,) and np.isfinite(w).all() and float(np.abs(w).max()) > 0
