@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-every", type=int, default=20)
     p.add_argument("--no-autotune", action="store_true", help="keep the default shots per block")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-vs-plain time-to-Vs-error measurement (N = 1 only)")
     return p.parse_args()
 
 
@@ -360,6 +362,10 @@ def main():
         v, dt = cpu_gradient_rate(cfg, nsh, 200, threads=ncores)
         cpu = {"value": v, "unit": UNIT, "cores": ncores, "kind": "port",
                "sample": f"{nsh} shots x 200 steps of the workload, oracle port FP32 ({dt:.1f} s)"}
+    S.close()
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_vs_plain()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -369,11 +375,43 @@ def main():
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": launches, "clocks": clocks,
-                "misfit": float(mis_d.sum().item())}
+                "misfit": float(mis_d.sum().item()),
+                "learned_vs_plain": learned}
         print(json.dumps(line), flush=True)
-    S.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def learned_vs_plain(seeds=(5000, 5001, 5002, 5003)):
+    """The metric's second half, after the timed region: wall time for the
+    learned preconditioner (shipped U-Net, tcgen05 kernels) to reach the Vs
+    relative-RMS error that plain illumination-preconditioned L-BFGS reaches
+    in 20 iterations, over the plain method's time, on held-out seeded
+    models (10 shots, 152 x 500, 3 Hz band; four models in lockstep)."""
+    import torch
+    try:
+        from stfwi_b200.learned import UNet, padded_shape
+        from stfwi_b200.learned import experiment as E
+        from stfwi_b200.learned.unet import load_weights
+        torch.cuda.empty_cache()
+        h, w = padded_shape(152, 500)
+        net = UNet(h, w)
+        weights = os.path.join(ROOT, "stfwi_b200", "learned", "weights", "unet_152x500_3hz.npz")
+        net.load_state_dict({"params": load_weights(weights), "h": h, "w": w})
+        recs = E.evaluate(net, list(seeds), K=4, n_plain=20, log=lambda m: None)
+        s = E.summarize(recs)
+        return {"metric": "time to the plain method's Vs relative-RMS error, learned / plain",
+                "median_time_ratio": s["median_time_ratio"], "mean_time_ratio": s["mean_time_ratio"],
+                "models": s["models"], "reached_target": s["reached_target"],
+                "learned_step_accepted": s["learned_step_accepted"],
+                "plain_time_s": [r["plain_time_s"] for r in recs],
+                "learned_time_s": [r["learned_time_s"] for r in recs],
+                "target_vs_rel_rms": [r["target"] for r in recs],
+                "config": {"workload": "held-out layered-fault models (seeds %d-%d), 152x500, 10 shots, "
+                                       "3 Hz band, known Vp and density; plain = 20 L-BFGS iterations"
+                                       % (seeds[0], seeds[-1])}}
+    except Exception as e:  # the Gcell/s line stands on its own
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 if __name__ == "__main__":
