@@ -29,7 +29,7 @@ import time
 import numpy as np
 
 from . import inversion as I
-from .unet import UNet, padded_shape, save_weights
+from .unet import UNet, load_weights, padded_shape, save_weights
 
 TARGET_SCALE = 100.0      # m/s per unit of the network's output
 
@@ -254,6 +254,8 @@ def main(argv=None):
     ap.add_argument("--val", type=int, default=16, help="training pairs held out for validation")
     ap.add_argument("--K", type=int, default=4, help="models evaluated concurrently")
     ap.add_argument("--out", default="learned_out")
+    ap.add_argument("--weights", default=None,
+                    help="evaluate these trained weights (save_weights format) instead of generating data and training")
     a = ap.parse_args(argv)
     os.makedirs(a.out, exist_ok=True)
     logf = open(os.path.join(a.out, "log.txt"), "a")
@@ -263,13 +265,20 @@ def main(argv=None):
         logf.write(msg + "\n")
         logf.flush()
 
-    X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log)
-    n_val = min(a.val, X.shape[0] // 4)
-    t0 = time.perf_counter()
-    net, hist, best_epoch = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
-    t_train = time.perf_counter() - t0
-    zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
-    save_weights(os.path.join(a.out, "unet_weights.npz"), net.params.detach().cpu().numpy())
+    if a.weights:
+        h, w = padded_shape(I.GEOMETRY["nz"], I.GEOMETRY["nx"])
+        net = UNet(h, w)
+        net.load_state_dict({"params": load_weights(a.weights), "h": h, "w": w})
+        t_data = t_train = 0.0
+        hist, best_epoch, zero_val = [], None, None
+    else:
+        X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log)
+        n_val = min(a.val, X.shape[0] // 4)
+        t0 = time.perf_counter()
+        net, hist, best_epoch = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
+        t_train = time.perf_counter() - t0
+        zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
+        save_weights(os.path.join(a.out, "unet_weights.npz"), net.params.detach().cpu().numpy())
     recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
     summary = dict(config=dict(vars(a), geometry=I.GEOMETRY), data_seconds=t_data, train_seconds=t_train,
                    train_history=hist, best_epoch=best_epoch, val_loss_of_zero_prediction=zero_val,
