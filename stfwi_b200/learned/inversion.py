@@ -68,7 +68,9 @@ def lbfgs(vs0, vp, precond, n_iter, mem=10, step0=50.0, c1=1e-4, max_ls=6, recor
     g_Vs).  The first direction is the preconditioned steepest descent scaled
     to a largest change of ``step0`` m/s; later ones come from the two-loop
     recursion over the last ``mem`` pairs; each step backtracks (halving)
-    until the Armijo condition holds.  ``record(vs, f, g_raw)`` is called on
+    until the Armijo condition holds; when ``max_ls`` halvings find no
+    decrease the memory is cleared and the next iteration restarts from the
+    scaled steepest descent (the iteration stops only when that fails too).  ``record(vs, f, g_raw)`` is called on
     every accepted iterate (and the start); the iteration ends early when
     ``stop(vs, f)`` is true there.  Returns the final Vs."""
     vp = np.asarray(vp, np.float64)
@@ -109,6 +111,9 @@ def lbfgs(vs0, vp, precond, n_iter, mem=10, step0=50.0, c1=1e-4, max_ls=6, recor
                 break
             alpha *= 0.5
         if not accepted:
+            if S:                                # stale curvature pairs: restart
+                S, Y = [], []
+                continue
             return x
         gn = graw * P
         s, y = xn - x, gn - g

@@ -54,3 +54,41 @@ def test_lbfgs_stops_when_asked():
                 record=lambda x, f, g: seen.append(f), stop=lambda x, f: f < 1e4)
     run_lockstep(batch, [gen])
     assert seen[-1] < 1e4 and all(f >= 1e4 for f in seen[:-1])
+
+
+def test_lbfgs_restarts_after_a_failed_line_search():
+    """A pseudo-Huber misfit is almost linear far from its minimum, so the
+    curvature pairs gathered there make the two-loop step overshoot far
+    beyond what the halvings repair; the iteration then restarts from the
+    scaled steepest descent instead of stopping."""
+    from stfwi_b200.learned.inversion import lbfgs
+
+    shape = (3, 3)
+
+    def ev(x):
+        r = x - 1800.0
+        return float(np.sum(np.sqrt(1.0 + r * r) - 1.0)), r / np.sqrt(1.0 + r * r)
+
+    n_eval = [0]
+    accepted = []
+    gen = lbfgs(np.full(shape, 1500.0), np.full(shape, 3000.0), np.ones(shape), n_iter=30, step0=10.0,
+                max_ls=3, record=lambda x, f, g: accepted.append((n_eval[0], f)))
+    x = next(gen)
+    run = longest = 0
+    restarted_then_accepted = False
+    try:
+        while True:
+            before = len(accepted)
+            n_eval[0] += 1
+            x = gen.send(ev(x))
+            if len(accepted) > before:
+                restarted_then_accepted |= run >= 3
+                run = 0
+            else:
+                run += 1
+                longest = max(longest, run)
+    except StopIteration:
+        pass
+    assert longest >= 3 and restarted_then_accepted
+    fs = [f for _, f in accepted]
+    assert fs[-1] < 0.5 * fs[0] and all(b <= a for a, b in zip(fs, fs[1:]))
