@@ -641,14 +641,36 @@ int check_launch(const char *what)
     return STFWI_OK;
 }
 
+constexpr int NN_MAX_DEVICES = 64;
+
+// one pipeline error flag per device (a kernel writes the flag of its own device)
 int *err_flag()
 {
-    static int *flag = nullptr;
-    if (!flag) {
-        if (cudaMalloc(&flag, sizeof(int)) != cudaSuccess) return nullptr;
-        cudaMemset(flag, 0, sizeof(int));
+    static int *flags[NN_MAX_DEVICES] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NN_MAX_DEVICES) return nullptr;
+    if (!flags[dev]) {
+        int *f = nullptr;
+        if (cudaMalloc(&f, sizeof(int)) != cudaSuccess) return nullptr;
+        cudaMemset(f, 0, sizeof(int));
+        flags[dev] = f;
     }
-    return flag;
+    return flags[dev];
+}
+
+// the dynamic shared-memory limit of a kernel is set once per device
+template <typename K>
+int smem_limit_once(K kern, size_t bytes, bool (&done)[NN_MAX_DEVICES], const char *what)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NN_MAX_DEVICES)
+        return nn_fail(STFWI_ERR_CUDA, "%s: no usable current device", what);
+    if (!done[dev]) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+            return check_launch(what);
+        done[dev] = true;
+    }
+    return STFWI_OK;
 }
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -710,13 +732,9 @@ int conv_common(const void *x, int n, int h, int w, int cin, const void *wt, int
     if (rc) return rc;
     int *err = err_flag();
     if (!err) return nn_fail(STFWI_ERR_OOM, "conv: error flag allocation failed");
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_conv_kmajor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem(64, 128)) !=
-            cudaSuccess)
-            return check_launch("conv: shared-memory attribute");
-        attr = true;
-    }
+    static bool attr[NN_MAX_DEVICES] = {};
+    rc = smem_limit_once(k_conv_kmajor, conv_smem(64, 128), attr, "conv: shared-memory attribute");
+    if (rc) return rc;
     const dim3 grid((unsigned)((size_t)n * (h / g.bh) * (w / g.bw)), (unsigned)(cout / g.bn));
     k_conv_kmajor<<<grid, CONV_THREADS, conv_smem(g.kc, g.bn), st>>>(
         tx, tw, g, bias, static_cast<const __nv_bfloat16 *>(mask), static_cast<__nv_bfloat16 *>(y), err);
@@ -800,13 +818,9 @@ int stfwi_nn_conv3x3_wgrad(const void *x, const void *dz, int n, int h, int w, i
     if (rc) return rc;
     int *err = err_flag();
     if (!err) return nn_fail(STFWI_ERR_OOM, "wgrad: error flag allocation failed");
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_conv_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgrad_smem(128)) !=
-            cudaSuccess)
-            return check_launch("wgrad: shared-memory attribute");
-        attr = true;
-    }
+    static bool attr[NN_MAX_DEVICES] = {};
+    rc = smem_limit_once(k_conv_wgrad, wgrad_smem(128), attr, "wgrad: shared-memory attribute");
+    if (rc) return rc;
     const dim3 grid((unsigned)splits, (unsigned)(co_tiles * g.ci_tiles), 9);
     k_conv_wgrad<<<grid, CONV_THREADS, wgrad_smem(g.bn), static_cast<cudaStream_t>(stream)>>>(ta, tb, g, dw, err);
     return check_launch("k_conv_wgrad");
