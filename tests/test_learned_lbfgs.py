@@ -92,3 +92,39 @@ def test_lbfgs_restarts_after_a_failed_line_search():
     assert longest >= 3 and restarted_then_accepted
     fs = [f for _, f in accepted]
     assert fs[-1] < 0.5 * fs[0] and all(b <= a for a, b in zip(fs, fs[1:]))
+
+
+def test_experiment_features_and_summary():
+    """Network input normalisation, the time-to-target rule and the summary."""
+    from stfwi_b200.learned import experiment as E
+    rng = np.random.default_rng(4)
+    g = rng.standard_normal((6, 9))
+    P = rng.uniform(0, 1, (6, 9))
+    vp = np.full((6, 9), 4000.0)
+    vs = np.full((6, 9), 2200.0)
+    f = E.features(g, P, vp, vs)
+    assert f.shape == (4, 6, 9) and f.dtype == np.float32
+    assert abs(float(np.abs(f[0]).max()) - 1.0) < 1e-6               # preconditioned gradient over its max
+    assert np.allclose(f[0], (g * P) / np.abs(g * P).max(), atol=1e-6)
+    assert np.allclose(f[1], P) and np.allclose(f[2], 1.0) and np.allclose(f[3], 1.0)
+    hist = [(0.5, 0.060, 9.0), (1.0, 0.055, 8.0), (1.5, 0.050, 7.0), (2.0, 0.052, 6.9)]
+    assert E._first_time(hist, 0.055) == 1.0 and E._first_time(hist, 0.049) is None
+    recs = [dict(ratio=0.2, learned_time_s=1.0, learned_step_accepted=True, err_start=0.06, target=0.05,
+                 err_after_learned_step=0.052),
+            dict(ratio=None, learned_time_s=None, learned_step_accepted=False, err_start=0.07, target=0.06,
+                 err_after_learned_step=None),
+            dict(ratio=0.6, learned_time_s=3.0, learned_step_accepted=True, err_start=0.05, target=0.049,
+                 err_after_learned_step=0.0495)]
+    s = E.summarize(recs)
+    assert s["models"] == 3 and s["reached_target"] == 2 and s["learned_step_accepted"] == 2
+    assert abs(s["median_time_ratio"] - 0.4) < 1e-12 and abs(s["median_err_after_learned_step"] - 0.05075) < 1e-12
+
+
+def test_acquisition_and_model_pair():
+    from stfwi_b200.learned import inversion as I
+    sx, sz, types, rx, rz = I.acquisition()
+    assert sx.size == 10 and sx.min() >= 0 and sx.max() < 500 and np.all(np.diff(sx) == 50)
+    assert types[:2] == ["force", "moment"] and rx.size == 250 and np.all(rz == 1)
+    (vs, vp, rho), (vs0, vp0, rho0) = I.true_and_initial(5000)
+    assert vs.shape == (152, 500) and np.all(vs <= vp / 1.2 + 1e-3)
+    assert I.vs_rel_rms(vs, vs) == 0.0 and 0.0 < I.vs_rel_rms(vs0, vs) < 0.2
