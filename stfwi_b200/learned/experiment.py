@@ -258,8 +258,11 @@ def main(argv=None):
                     help="evaluate these trained weights (save_weights format) instead of generating data and training")
     a = ap.parse_args(argv)
     os.makedirs(a.out, exist_ok=True)
-    logf = open(os.path.join(a.out, "log.txt"), "a")
+    with open(os.path.join(a.out, "log.txt"), "a") as logf:
+        _run(a, logf)
 
+
+def _run(a, logf):
     def log(msg):
         print(msg, flush=True)
         logf.write(msg + "\n")
