@@ -76,7 +76,7 @@ def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
     return np.stack(X), np.stack(Y), time.perf_counter() - t0
 
 
-def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
+def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print, device="cuda"):
     """Adam with a cosine learning-rate decay on the pairs (and their
     mirror images); the last ``n_val`` pairs are held out as validation and
     the weights of the epoch with the lowest validation loss are kept.
@@ -85,11 +85,12 @@ def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
     n_all, _, nz, nx = X.shape
     n = n_all - n_val
     h, w = padded_shape(nz, nx)
-    net = UNet(h, w, seed=seed)
-    Xd = torch.from_numpy(np.ascontiguousarray(X[:n])).cuda()
-    Yd = torch.from_numpy(np.ascontiguousarray(Y[:n])).cuda()
-    tgt = torch.zeros((batch, h, w), device="cuda")
-    wgt = torch.zeros((batch, h, w), device="cuda")
+    net = UNet(h, w, seed=seed, device=device)
+    dev = net.device
+    Xd = torch.from_numpy(np.ascontiguousarray(X[:n])).to(dev)
+    Yd = torch.from_numpy(np.ascontiguousarray(Y[:n])).to(dev)
+    tgt = torch.zeros((batch, h, w), device=dev)
+    wgt = torch.zeros((batch, h, w), device=dev)
     wgt[:, :nz, :nx] = 1.0
     inv = 1.0 / (batch * nz * nx)
     rng = np.random.default_rng(seed)
@@ -100,9 +101,9 @@ def train(X, Y, epochs=60, batch=8, lr=1e-3, seed=0, n_val=0, log=print):
     best = (float("inf"), -1, None)
     for ep in range(epochs):
         perm = rng.permutation(2 * n)
-        acc = torch.zeros(1, dtype=torch.float64, device="cuda")
+        acc = torch.zeros(1, dtype=torch.float64, device=dev)
         for b0 in range(0, per_epoch * batch, batch):
-            idx = torch.from_numpy(perm[b0:b0 + batch]).cuda()
+            idx = torch.from_numpy(perm[b0:b0 + batch]).to(dev)
             src, flip = idx % n, (idx >= n)
             xb, yb = Xd[src], Yd[src]
             xb = torch.where(flip[:, None, None, None], xb.flip(-1), xb)
@@ -130,7 +131,7 @@ def predict(net, X, batch=8):
     n, _, nz, nx = X.shape
     out = []
     for b0 in range(0, n, batch):
-        xb = torch.from_numpy(np.ascontiguousarray(X[b0:b0 + batch])).cuda()
+        xb = torch.from_numpy(np.ascontiguousarray(X[b0:b0 + batch])).to(net.device)
         o = net.forward(net.pack(xb))
         out.append(o[:, :nz, :nx].cpu().numpy())
     return np.concatenate(out)

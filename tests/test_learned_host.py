@@ -111,3 +111,26 @@ def test_compact_weights_keep_what_the_kernels_read(tmp_path):
     shipped = os.path.join(os.path.dirname(__file__), "..", "stfwi_b200", "learned", "weights", "unet_152x500_3hz.npz")
     w = load_weights(shipped)
     assert w.shape == (total,) and np.isfinite(w).all() and float(np.abs(w).max()) > 0
+
+
+def test_training_loop_keeps_the_best_validation_weights(monkeypatch):
+    """experiment.train on the CPU stand-in of the kernels: mirror-image
+    augmentation, the cosine schedule, and the weights of the epoch with
+    the lowest validation loss restored at the end."""
+    import torch
+    from stfwi_b200 import _native as N
+    from stfwi_b200.learned import experiment as E
+    from stfwi_b200.learned import unet as U
+    from tests.fake_nn import FakeNN
+    monkeypatch.setattr(N, "load", lambda: FakeNN())
+    monkeypatch.setattr(U, "_p", lambda t: t)
+    monkeypatch.setattr(U.UNet, "storage_dtype", torch.float64)
+    rng = np.random.default_rng(7)
+    X = rng.standard_normal((6, 4, 14, 500)).astype(np.float32)
+    Y = (0.5 * X[:, 0] + 0.1).astype(np.float32)
+    logs = []
+    net, hist, best = E.train(X, Y, epochs=2, batch=4, lr=1e-3, n_val=2, log=logs.append, device="cpu")
+    assert len(hist) == 2 and len(logs) == 2 and 1 <= best <= 2
+    vals = [v for _, v in hist]
+    assert abs(E.validation_loss(net, X[4:], Y[4:], batch=4) - min(vals)) < 1e-9 * max(min(vals), 1.0)
+    assert net.step_count == 2 * ((2 * 4) // 4)          # steps per epoch over the data and its mirror images
