@@ -14,7 +14,8 @@
  * 3x3 weights are BF16 [9][cout][cin] with tap = 3*(dy+1) + (dx+1)
  * (output pixel p reads input pixel p + (dy, dx)); convolutions are
  * stride 1 with zero padding 1; channel counts are multiples of 16. All
- * pointers are device memory, 16-byte aligned; every call is asynchronous
+ * tensor pointers are device memory, 16-byte aligned (scale4 of
+ * stfwi_nn_pack_input is host memory); every call is asynchronous
  * on `stream` (a cudaStream_t, NULL = default stream). Status codes are
  * those of stfwi.h; stfwi_nn_last_error() gives the message of the last
  * failing call of this thread. stfwi_nn_check() synchronises the stream and
@@ -48,7 +49,8 @@ int stfwi_nn_conv3x3_dgrad(const void *dz, int n, int h, int w, int cout, const 
 int stfwi_nn_conv3x3_wgrad(const void *x, const void *dz, int n, int h, int w, int cin, int cout, float *dw,
                            void *stream);
 
-/* features [n][4][hd][wd] FP32 times scale4[c] -> x [n][h][w][16] BF16, zero outside hd x wd and in channels 4-15 */
+/* features [n][4][hd][wd] FP32 times scale4[c] (4 floats, host) -> x [n][h][w][16] BF16, zero outside
+   hd x wd and in channels 4-15 */
 int stfwi_nn_pack_input(const float *feat, int n, int hd, int wd, int h, int w, const float *scale4, void *x,
                         void *stream);
 
