@@ -1,6 +1,6 @@
 """A small, self-contained run of the batched gradient for profiling.
 
-    python -m stfwi_b200.profile_case --shots 50 --nt 40
+    python -m benchmarks.profile_case --shots 50 --nt 40
 
 Runs the batched-shot workload (152 x 500 layered-fault model, fd 8, free
 surface) with `shots` shots for `nt` steps: forward with history, misfit,

@@ -3,14 +3,14 @@
 (forward, loss, backward, Adam) at a batch of 8, timed with CUDA events on
 the launching stream, and the convolutions' dense FLOP rate.
 
-    python -m stfwi_b200.learned.profile_net [--batch 8] [--steps 20] [--warmup 3]
+    python -m benchmarks.profile_net [--batch 8] [--steps 20] [--warmup 3]
 """
 from __future__ import annotations
 
 import argparse
 import json
 
-from .unet import LAYERS, UNet, padded_shape
+from stfwi_b200.learned.unet import LAYERS, UNet, padded_shape
 
 
 def conv_flops(h, w, batch):

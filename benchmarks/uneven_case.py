@@ -4,7 +4,7 @@
 exact gradient per model, first one model at a time, then all models with
 their launches interleaved on separate streams.
 
-    python -m stfwi_b200.uneven_case [--scale 1.0]
+    python -m benchmarks.uneven_case [--scale 1.0]
 
 ``--scale`` shrinks the step counts (a quick run); the printed JSON line
 holds per-model and whole-batch fwd+adj Gcell-updates/s.
@@ -17,7 +17,7 @@ import numpy as np
 
 
 def specs(scale=1.0):
-    from . import models as Mo
+    from stfwi_b200 import models as Mo
     out = []
     # memory budgets (GB): store-all history for the small grid, checkpoint
     # segments chosen by the handle for the two larger ones (180 GB in all)
@@ -41,7 +41,7 @@ def main():
     p.add_argument("--scale", type=float, default=1.0)
     a = p.parse_args()
     import torch
-    from .batch import UnevenBatch
+    from stfwi_b200.batch import UnevenBatch
     sp = specs(a.scale)
     torch.cuda.init()
     B = UnevenBatch(sp)

@@ -83,17 +83,19 @@ typedef struct {
 #define STFWI_GRAD_IMAGING 2u /* the reference's continuous imaging formula */
 #define STFWI_GRAD_SRC 4u     /* source-wavelet adjoint (dot-product test) */
 
-/* Residual preparation: misfit_k = scale/nshot * mean_{t,r}(F T (pred - obs))^2
+/* Residual preparation: misfit_k = scale/N * mean_{t,r}(F T (pred - obs))^2
  * on one receiver component; F = cascade of nsos biquads (b0 b1 b2 a0 a1 a2,
  * scipy 'sos' layout, normalised by a0), T = cosine end taper of n_taper
- * samples (fwi/filters.py). */
+ * samples (fwi/filters.py).  N = nshot_norm when it is > 0, else the number
+ * of shots of the call; the adjoint sources carry the same 1/N. */
 typedef struct {
-    int32_t component; /* 0 vx, 1 vz, 2 exx, 3 ezz */
+    int32_t component;  /* 0 vx, 1 vz, 2 exx, 3 ezz */
     int32_t n_taper;
-    int32_t nsos;      /* 0: no filter; at most 16 sections */
-    int32_t reserved;
+    int32_t nsos;       /* 0: no filter; at most 16 sections */
+    int32_t nshot_norm; /* 0: the call's own shot count; > 0: the total number of
+                           shots across the ranks that share one loss (sharding) */
     double scale;
-    const double *sos; /* host pointer, [nsos][6] */
+    const double *sos;  /* host pointer, [nsos][6] */
 } stfwi_misfit_desc;
 
 /* Device bytes stfwi_create allocates for d (with ckpt_interval = 0: the
@@ -134,8 +136,10 @@ stfwi_status stfwi_set_adjoint_sources(stfwi_handle *h, const float *rec_adj, vo
 
 /* Adjoint sweep.  mode: STFWI_GRAD_* bits.  g_out: for each of EXACT then
  * IMAGING that is set, [3][nz_dom][nx_dom] FP64 = (dJ/dVs, dJ/dVp, dJ/drho)
- * summed over shots (dJ/drho is only filled by IMAGING's Lame part; EXACT
- * returns it as 0).  src_wav_a: [nshot][nt] float32 when SRC is set. */
+ * summed over shots.  dJ/drho is filled by both modes when the handle was
+ * created with want_gradient = 2 (the history then holds the velocities the
+ * density term needs); with want_gradient = 1 both modes return it as 0.
+ * src_wav_a: [nshot][nt] float32 when SRC is set. */
 stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float *src_wav_a,
                             void *stream);
 
@@ -170,15 +174,19 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
  * reference): the same misfit and adjoint sources as stfwi_misfit, without a
  * handle, for callers that cannot call cudaMalloc -- e.g. a custom call made
  * from inside a framework that has reserved most of device memory for its own
- * pool, or code recording a stream capture.  All pointers are device memory:
+ * pool, where one more allocation can fail or fragment that pool.  All
+ * pointers are device memory:
  * pred [nshot][4][nt][nrec] (the layout stfwi_get_records returns), obs
  * [nshot][nt][nrec], rec_adj [nshot][4][nt][nrec] (written), misfit_out
  * [nshot] FP64 (written).  Its only scratch is a fixed device array of
  * 262144 FP64 per-trace sums (2 MiB, held by every GPU that loads the library
  * until exit): nshot * nrec above that limit returns STFWI_ERR_INVALID.  The
- * first call on a device looks the array up (cudaGetSymbolAddress) and should
- * come before any stream capture on that device.  Calls share the array, so
- * calls that overlap on the GPU race.  Errors are printed to stderr. */
+ * first call on a device (and the first after that device's context was
+ * replaced, e.g. by cudaDeviceReset) looks the array up with
+ * cudaGetSymbolAddress; make that first call before any stream capture on
+ * the device.  Every slot of the array is written before it is read, and all
+ * calls share it, so calls that overlap on the GPU race.  It calls no
+ * cudaMalloc or cudaFree.  Errors are printed to stderr. */
 stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t nrec, const float *pred,
                                   const float *obs, const stfwi_misfit_desc *m, float *rec_adj,
                                   double *misfit_out, void *stream);

@@ -56,7 +56,7 @@ class StfwiDesc(ct.Structure):
 class StfwiMisfitDesc(ct.Structure):
     _fields_ = [
         ("component", ct.c_int32), ("n_taper", ct.c_int32), ("nsos", ct.c_int32),
-        ("reserved", ct.c_int32), ("scale", ct.c_double), ("sos", ct.POINTER(ct.c_double)),
+        ("nshot_norm", ct.c_int32), ("scale", ct.c_double), ("sos", ct.POINTER(ct.c_double)),
     ]
 
 

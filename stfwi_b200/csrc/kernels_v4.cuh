@@ -11,7 +11,7 @@
 #pragma once
 #include <type_traits>
 
-#include "kernels_v3.cuh"
+#include "common.cuh"
 
 namespace stfwi {
 

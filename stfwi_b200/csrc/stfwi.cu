@@ -16,8 +16,6 @@
 #include <vector>
 
 #include "../../include/stfwi.h"
-#include "kernels.cuh"
-#include "kernels_v3.cuh"
 #include "kernels_v4.cuh"
 #include "post.cuh"
 
@@ -45,7 +43,6 @@ struct stfwi_handle {
     stfwi_desc d{};
     Geo g{};
     int device = 0;
-    int groups = 1, spg = 1;  // shot groups per launch, shots per group
     std::string err;
 
     // model
@@ -55,16 +52,15 @@ struct stfwi_handle {
     float *vpmax = nullptr;
     float *MATS = nullptr;  // [4][nz][P]: B, L2M, L, M
     bool model_set = false;
-    // TMA-pipelined variant: tensor maps and per-kernel shot groups
-    int variant = 0, sms = 148;
+    // tensor maps of the staged tiles and per-kernel shot groups
+    int sms = 148;
     int accp = 5;   // accumulator planes per shot group (7 with the density terms)
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
     CUtensorMap tmUo{}, tmSo{}, tmPQo{}, tmEo{};   // own-cell boxes of the two-column kernels
     CUtensorMap tmH{};        // history [shot][slot*snf + field][nz_dom][nx_dom] (own-cell carry-in boxes)
     bool hist_tma = false;    // tmH valid: pad and nx_dom multiples of 4 (16-byte box rows)
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
-    // rows high, adj_b tiles thb rows high (variant 0: 64 x 32 and 64 x 16;
-    // variant 2: 32 x 8*RPT3 and 32 x 32)
+    // rows high, adj_b tiles thb rows high
     int tw = TX4, tha = RPT4 * NWARP, thb = RPT4B * NWARP;
     int ntx = 1, ntza = 1, ntzb = 1;                       // tile counts
     int *tile_startA = nullptr, *tile_recA = nullptr;      // receivers grouped by the tw x tha tiles
@@ -79,7 +75,7 @@ struct stfwi_handle {
     int nshot = 0;
     int *sx = nullptr, *sz = nullptr, *stype = nullptr;
     float *wav = nullptr, *fcoef = nullptr, *mcoef = nullptr, *lm = nullptr;
-    int *tile_start = nullptr, *tile_rec = nullptr, *rx = nullptr, *rz = nullptr;
+    int *rx = nullptr, *rz = nullptr;
     bool shots_set = false, recv_set = false;
     std::vector<int> rec_x_h, rec_z_h;   // physical-domain receiver indices (preconditioner geometry)
 
@@ -146,18 +142,16 @@ stfwi_status fail(stfwi_handle *h, stfwi_status st, const char *fmt, ...)
 
 struct Plan {
     long long nz, nx, P, nd, zs_n, xs_n;
-    int tiles_x, tiles_z;
     size_t fields, psi, snap, row0, acc, rec, misc, ckpt;
     size_t total() const { return fields + psi + snap + row0 + acc + rec + misc + ckpt; }
 };
 
-int auto_groups(const stfwi_desc *d, int tiles)
+// FP64 gradient accumulator groups: one per group of shots of the strain
+// phase, at least two shots per group unless the descriptor asks otherwise
+int acc_groups_of(const stfwi_desc *d)
 {
-    if (d->shot_group > 0) return std::max(1, (d->max_shots + d->shot_group - 1) / d->shot_group);
-    // enough blocks to fill 148 SMs a few times over, few enough that each
-    // block reuses its material tile and gradient registers across shots
-    int want = std::max(1, (4 * 148 + tiles - 1) / tiles);
-    return std::min(want, std::max(1, d->max_shots));
+    const int spg0 = d->shot_group > 0 ? d->shot_group : 2;
+    return std::max(1, (d->max_shots + spg0 - 1) / spg0);
 }
 
 // k: history segment length (k = nt: every step kept, no checkpoints)
@@ -170,10 +164,8 @@ Plan make_plan(const stfwi_desc *d, int k)
     p.nd = (long long)d->nz_dom * d->nx_dom;
     p.xs_n = 2LL * d->pad;
     p.zs_n = d->free_surface ? d->pad : 2LL * d->pad;
-    p.tiles_x = (int)((p.nx + TX - 1) / TX);
-    p.tiles_z = (int)((p.nz + TZ - 1) / TZ);
     const long long S = d->max_shots;
-    const int G = auto_groups(d, p.tiles_x * p.tiles_z);
+    const int G = acc_groups_of(d);
     p.fields = (size_t)2 * S * F_N * p.nz * p.P * sizeof(float);
     p.psi = (size_t)S * (NPX * p.nz * p.xs_n + NPZ * p.zs_n * p.P) * sizeof(float);
     // history fields per slot: the stresses, plus U and V for the density
@@ -413,7 +405,6 @@ Shots shots_of(stfwi_handle *h)
 {
     return Shots{h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef, h->lm};
 }
-Recv recv_of(stfwi_handle *h) { return Recv{h->tile_start, h->tile_rec, h->rx, h->rz}; }
 
 // event pair of sampled step n around kernel k (0 fwd_vel, 1 fwd_str, 2 adj_a, 3 adj_b)
 inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
@@ -430,41 +421,8 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
 }
 
 template <int FD>
-void launch_fwd_step_plain(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
-{
-    // one shot per block: the forward carries no cross-shot state (the
-    // illumination sum uses FP64 atomics per cell and shot)
-    dim3 grid(h->g.tiles_x * h->g.tiles_z, h->nshot), block(TX, NWARP);
-    prof_mark(h, 0, n, 0, st);
-    k_fwd_vel<FD><<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, 1);
-    prof_mark(h, 0, n, 1, st);
-    prof_mark(h, 1, n, 0, st);
-    k_fwd_str<FD><<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->F, h->PX, h->PZ,
-                                          n, 1, o);
-    prof_mark(h, 1, n, 1, st);
-}
-
-template <int FD>
-void launch_fwd_step_v3(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
-{
-    const int tiles = h->ntx * h->ntza;
-    dim3 block(TX, NWARP);
-    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    prof_mark(h, 0, n, 0, st);
-    k3_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L3<FD>::bytes(L3<FD>::VEL, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS);
-    prof_mark(h, 0, n, 1, st);
-    prof_mark(h, 1, n, 0, st);
-    k3_fwd_str<FD><<<dim3(tiles, h->grp[1]), block, L3<FD>::bytes(L3<FD>::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV);
-    prof_mark(h, 1, n, 1, st);
-}
-
-template <int FD>
 void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
-    if (h->variant == 1) return launch_fwd_step_plain<FD>(h, n, o, st);
-    if (h->variant == 2) return launch_fwd_step_v3<FD>(h, n, o, st);
     const int tiles = h->ntx * h->ntza;
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
@@ -480,60 +438,8 @@ void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 }
 
 template <int FD>
-void launch_adj_step_plain(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
-{
-    // U_a/V_a phase: one shot per block (no cross-shot state); strain phase:
-    // shot groups, so the FP64 gradient sum over shots stays in registers
-    dim3 grid_a(h->g.tiles_x * h->g.tiles_z, h->nshot), grid(h->g.tiles_x * h->g.tiles_z, h->groups);
-    dim3 block(TX, NWARP);
-    prof_mark(h, 2, n, 0, st);
-    k_adj_a<FD><<<grid_a, block, 0, st>>>(h->g, mat_of(h), recv_of(h), h->A, h->PX, h->PZ, n, 1, ai);
-    prof_mark(h, 2, n, 1, st);
-    prof_mark(h, 3, n, 0, st);
-    auto args = [&](auto kern) {
-        kern<<<grid, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX, h->PZ, n, h->spg, ao);
-    };
-    if (ao.want_exact && ao.want_img) args(k_adj_b<FD, true, true>);
-    else if (ao.want_exact) args(k_adj_b<FD, true, false>);
-    else if (ao.want_img) args(k_adj_b<FD, false, true>);
-    else {
-        dim3 grid1(h->g.tiles_x * h->g.tiles_z, h->nshot);
-        k_adj_b<FD, false, false><<<grid1, block, 0, st>>>(h->g, mat_of(h), shots_of(h), recv_of(h), h->A, h->PX,
-                                                          h->PZ, n, 1, ao);
-    }
-    prof_mark(h, 3, n, 1, st);
-}
-
-
-
-template <int FD>
-void launch_adj_step_v3(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
-{
-    dim3 block(TX, NWARP);
-    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
-    prof_mark(h, 2, n, 0, st);
-    k3_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L3<FD>::bytes(L3<FD>::ADA, 2), st>>>(
-        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE);
-    prof_mark(h, 2, n, 1, st);
-    prof_mark(h, 3, n, 0, st);
-    auto launch = [&](auto kern) {
-        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L3<FD>::bytes(L3<FD>::ADB, 2), st>>>(
-            h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
-            h->tmPQ);
-    };
-    if (ao.want_exact && ao.want_img) launch(k3_adj_b<FD, true, true>);
-    else if (ao.want_exact) launch(k3_adj_b<FD, true, false>);
-    else if (ao.want_img) launch(k3_adj_b<FD, false, true>);
-    else launch(k3_adj_b<FD, false, false>);
-    prof_mark(h, 3, n, 1, st);
-}
-
-template <int FD>
 void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
 {
-    if (h->variant == 1) return launch_adj_step_plain<FD>(h, n, ai, ao, st);
-    if (h->variant == 2) return launch_adj_step_v3<FD>(h, n, ai, ao, st);
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
@@ -769,13 +675,6 @@ stfwi_status set_smem(stfwi_handle *h, const void *const (&kern)[7])
 template <int FD>
 stfwi_status setup_tma_kernels(stfwi_handle *h)
 {
-    if (h->variant == 2) {
-        const void *const kern[7] = {
-            (const void *)k3_fwd_vel<FD>, (const void *)k3_fwd_str<FD>, (const void *)k3_adj_a<FD>,
-            (const void *)k3_adj_b<FD, true, false>, (const void *)k3_adj_b<FD, true, true>,
-            (const void *)k3_adj_b<FD, false, true>, (const void *)k3_adj_b<FD, false, false>};
-        return set_smem<L3<FD>>(h, kern);
-    }
     const void *const kern[7] = {
         (const void *)k4_fwd_vel<FD>, (const void *)k4_fwd_str<FD, false>, (const void *)k4_adj_a<FD>,
         (const void *)k4_adj_b<FD, true, false, false>, (const void *)k4_adj_b<FD, true, true, false>,
@@ -810,7 +709,7 @@ stfwi_status setup_tensor_maps(stfwi_handle *h)
     if ((r = encode(h, &h->tmV, h->F, 4, fdims, fstr, box2))) return r;
     if ((r = encode(h, &h->tmE, h->A, 4, fdims, fstr, box3))) return r;
     if ((r = encode(h, &h->tmPQ, h->A, 4, fdims, fstr, box2s))) return r;
-    if (h->variant == 0) {
+    {
         const cuuint32_t own2[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->tha, 2, 1};
         const cuuint32_t own3[4] = {(cuuint32_t)h->tw, (cuuint32_t)h->tha, 3, 1};
         if ((r = encode(h, &h->tmUo, h->F, 4, fdims, fstr, own2))) return r;
@@ -874,8 +773,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     if (!d || !out) return STFWI_ERR_INVALID;
     *out = nullptr;
     if (d->fd_order != 2 && d->fd_order != 4 && d->fd_order != 8) return STFWI_ERR_UNSUPPORTED;
-    // the velocity history of the density gradient is written by the default kernels only
-    if (d->want_gradient == 2 && d->kernel_variant != 0) return STFWI_ERR_UNSUPPORTED;
+    // one kernel family: the field is kept for the ABI, other values are refused
+    if (d->kernel_variant != 0) return STFWI_ERR_UNSUPPORTED;
     if (d->want_gradient < 0 || d->want_gradient > 2) return STFWI_ERR_INVALID;
     const int H = d->fd_order / 2;
     if (d->nz_dom < 1 || d->nx_dom < 1 || d->pad < H || d->nt < 1 || d->nrec < 0 || d->max_shots < 1 ||
@@ -919,7 +818,6 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.fs = d->free_surface ? 1 : 0;
     g.xs_n = (int)p.xs_n; g.zs_n = (int)p.zs_n;
     g.nt = d->nt; g.nrec = d->nrec; g.nshot = 0;
-    g.tiles_x = p.tiles_x; g.tiles_z = p.tiles_z;
     g.dtdx = (float)(d->dt / d->dx); g.dtdz = (float)(d->dt / d->dz); g.dzdx = (float)(d->dz / d->dx);
     g.dt = (float)d->dt;
     g.inv2dx = (float)(1.0 / (2.0 * d->dx)); g.inv2dz = (float)(1.0 / (2.0 * d->dz));
@@ -927,19 +825,12 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
     g.snf = d->want_gradient == 2 ? 5 : 3;
     h->accp = g.snf == 5 ? 7 : 5;
-    h->groups = auto_groups(d, p.tiles_x * p.tiles_z);
-    h->spg = (d->max_shots + h->groups - 1) / h->groups;
-    h->variant = (d->kernel_variant == 1 || d->kernel_variant == 2) ? d->kernel_variant : 0;
-    if (h->variant == 2) {
-        h->tw = TX; h->tha = RPT3 * NWARP; h->thb = 4 * NWARP;
-    } else {
-        h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
-    }
+    h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
     h->ntx = (int)((p.nx + h->tw - 1) / h->tw);
     h->ntza = (int)((p.nz + h->tha - 1) / h->tha);
     h->ntzb = (int)((p.nz + h->thb - 1) / h->thb);
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
-    if (h->variant != 1) {
+    {
         stfwi_status r = STFWI_OK;
         switch (d->fd_order) {
         case 2: r = setup_tma_kernels<2>(h); break;
@@ -947,10 +838,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         default: r = setup_tma_kernels<8>(h); break;
         }
         if (r) { delete h; return r; }
-        const int spg0 = d->shot_group > 0 ? d->shot_group : 2;
-        h->acc_groups = std::max(1, (d->max_shots + spg0 - 1) / spg0);
-    } else {
-        h->acc_groups = h->groups;
+        h->acc_groups = acc_groups_of(d);
     }
     h->acc_used = h->acc_groups;
     h->slots = k + 1 + ((g.snf == 5 && h->ncp > 0) ? 1 : 0);
@@ -977,8 +865,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
           alloc((void **)&h->tile_recA, nrec * 4) &&
           alloc((void **)&h->tile_startB, ((size_t)h->ntx * h->ntzb + 1) * 4) &&
           alloc((void **)&h->tile_recB, nrec * 4);
-    ok &= alloc((void **)&h->tile_start, ((size_t)p.tiles_x * p.tiles_z + 1) * 4) &&
-          alloc((void **)&h->tile_rec, nrec * 4) && alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
+    ok &= alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
     ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
     ok &= alloc((void **)&h->PX, (size_t)S * NPX * p.nz * p.xs_n * 4) &&
           alloc((void **)&h->PZ, (size_t)S * NPZ * p.zs_n * p.P * 4);
@@ -1016,7 +903,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     cudaMemset(h->MATS, 0, (size_t)4 * NP * 4);
     cudaMemset(h->F, 0, (size_t)S * F_N * NP * 4);
     cudaMemset(h->A, 0, (size_t)S * F_N * NP * 4);
-    if (h->variant != 1) {
+    {
         stfwi_status r = setup_tensor_maps(h);
         if (r) {
             fprintf(stderr, "stfwi_create: %s\n", h->err.c_str());
@@ -1035,7 +922,7 @@ void stfwi_destroy(stfwi_handle *h)
     drop_graphs(h);
     void *bufs[] = {h->vs, h->vp, h->rho, h->MATS, h->Lr, h->bx, h->ax, h->ikx, h->bz,
                     h->az, h->ikz, h->vpmax, h->status, h->sx, h->sz, h->stype, h->wav, h->fcoef, h->mcoef,
-                    h->lm, h->tile_start, h->tile_rec, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
+                    h->lm, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
                     h->mis_trace, h->mis_shot, h->src_a, h->pw, h->ptaper, h->pillum, h->ptmp, h->pscr, h->pmax,
                     h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->CKF, h->CKPX,
@@ -1085,24 +972,16 @@ stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *r
     const Geo &g = h->g;
     if (nrec != g.nrec) return fail(h, STFWI_ERR_INVALID, "nrec %d != descriptor nrec %d", nrec, g.nrec);
     if (nrec > 0 && (!rec_x || !rec_z)) return fail(h, STFWI_ERR_INVALID, "null receiver array");
-    const int ntile = g.tiles_x * g.tiles_z;
-    std::vector<int> rx(std::max(nrec, 1)), rz(std::max(nrec, 1)), cnt(ntile + 1, 0), start(ntile + 1, 0),
-        list(std::max(nrec, 1));
+    std::vector<int> rx(std::max(nrec, 1)), rz(std::max(nrec, 1));
     for (int r = 0; r < nrec; ++r) {
         rx[r] = rec_x[r] + g.pad;
         rz[r] = rec_z[r] + g.z0;
         if (rx[r] < 0 || rx[r] >= g.nx || rz[r] < 0 || rz[r] >= g.nz)
             return fail(h, STFWI_ERR_INVALID, "receiver %d at (%d,%d) is outside the grid", r, rec_z[r], rec_x[r]);
-        cnt[(rz[r] / TZ) * g.tiles_x + rx[r] / TX]++;
     }
-    for (int t = 0; t < ntile; ++t) start[t + 1] = start[t] + cnt[t];
-    std::vector<int> fill(start.begin(), start.end() - 1);
-    for (int r = 0; r < nrec; ++r) list[fill[(rz[r] / TZ) * g.tiles_x + rx[r] / TX]++] = r;
     CK(h, cudaMemcpy(h->rx, rx.data(), rx.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->rz, rz.data(), rz.size() * 4, cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->tile_start, start.data(), start.size() * 4, cudaMemcpyHostToDevice));
-    CK(h, cudaMemcpy(h->tile_rec, list.data(), list.size() * 4, cudaMemcpyHostToDevice));
-    // the same grouping for the two staged tilings
+    // receivers grouped by the tiles of the two staged tilings
     auto group = [&](int th, int ntz, int *d_start, int *d_list) -> stfwi_status {
         const int ntl = h->ntx * ntz;
         std::vector<int> c(ntl + 1, 0), st(ntl + 1, 0), l(std::max(nrec, 1));
@@ -1149,22 +1028,16 @@ stfwi_status stfwi_set_shots(stfwi_handle *h, int32_t nshot, const int32_t *src,
     if (nshot != h->nshot) drop_graphs(h);
     h->nshot = nshot;
     g.nshot = nshot;
-    h->spg = std::max(1, (nshot + h->groups - 1) / h->groups);
-    if (h->variant != 1) {
+    {
         // shots per block by default (measured on B200, 50 shots of 172 x 540):
         // enough blocks to keep every SM busy, copies of the next shots in
         // flight while one computes; the strain phase keeps FP64 sums per cell
         // over its shots and gains from larger groups
-        static const int dflt4[4] = {3, 3, 3, 4}, dflt3[4] = {2, 2, 2, 2};
+        static const int dflt4[4] = {3, 3, 3, 4};
         int spg[4];
         for (int k = 0; k < 4; ++k)
-            spg[k] = h->d.shot_group > 0 ? h->d.shot_group
-                   : h->tuned[k] > 0    ? h->tuned[k]
-                                        : (h->variant == 0 ? dflt4[k] : dflt3[k]);
+            spg[k] = h->d.shot_group > 0 ? h->d.shot_group : h->tuned[k] > 0 ? h->tuned[k] : dflt4[k];
         set_groups(h, spg);
-    } else {
-        h->acc_used = h->groups;
-        h->lr_used = nshot;  // the plain U_a/V_a phase runs one shot per block row
     }
     h->shots_set = true;
     h->stored = false;
@@ -1232,7 +1105,7 @@ stfwi_status stfwi_misfit(stfwi_handle *h, const float *obs, const stfwi_misfit_
         sp.c[k][0] = s[0] / s[3]; sp.c[k][1] = s[1] / s[3]; sp.c[k][2] = s[2] / s[3];
         sp.c[k][3] = s[4] / s[3]; sp.c[k][4] = s[5] / s[3];
     }
-    const int nnorm = m->reserved > 0 ? m->reserved : h->nshot;
+    const int nnorm = m->nshot_norm > 0 ? m->nshot_norm : h->nshot;
     CK(h, cudaMemcpyAsync(h->obs, obs, (size_t)h->nshot * g.nt * g.nrec * 4, cudaMemcpyDefault, st));
     const int n = h->nshot * g.nrec, thr = 128;
     if (n > 0) {
@@ -1537,7 +1410,6 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
 {
     stfwi_status rc = ready(h);
     if (rc) return rc;
-    if (h->variant == 1) return fail(h, STFWI_ERR_UNSUPPORTED, "the plain kernels run one shot per block");
     const Geo &g = h->g;
     steps = std::max(2, std::min((int)steps, g.nt));
     CK(h, cudaStreamSynchronize((cudaStream_t)stream));
@@ -1628,16 +1500,38 @@ stfwi_status stfwi_check(stfwi_handle *h, void *stream)
 // Residual preparation without any allocation, for callers that must not
 // call cudaMalloc: an XLA custom call running inside a framework that has
 // already reserved most of the device memory for its own pool (the JAX
-// drivers of this workload run with 90 % preallocated), or code recording
-// into a stream capture.  The only scratch it needs, one FP64 partial sum
-// per trace, lives in this file-scope device array; every GPU that loads the
-// library holds it until the process exits.
+// drivers of this workload run with 90 % preallocated), where a further
+// cudaMalloc can fail or fragment the pool.  The only scratch it needs, one
+// FP64 partial sum per trace, lives in this file-scope device array; every
+// GPU that loads the library holds it until the process exits.
 static constexpr int STFWI_NOALLOC_MAX_TRACES = 1 << 18;  // nshot * nrec <= 262144 (2 MiB)
 static __device__ __align__(256) double g_noalloc_trace_sums[STFWI_NOALLOC_MAX_TRACES];
 
 namespace {
 std::mutex g_noalloc_mu;
-double *g_noalloc_ptr[256] = {nullptr};
+// device address of the scratch per device, valid for the context it was
+// looked up in (a reset device gets a new context and a fresh lookup)
+struct NoallocSlot {
+    void *ctx = nullptr;
+    double *ptr = nullptr;
+};
+NoallocSlot g_noalloc_slot[256];
+
+typedef int (*ctx_current_fn)(void **);
+ctx_current_fn ctx_current()
+{
+    static ctx_current_fn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<ctx_current_fn>(p);
+    }
+    return fn;
+}
 }  // namespace
 
 extern "C" stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t nrec, const float *pred,
@@ -1668,22 +1562,32 @@ extern "C" stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t 
         sp.c[k][0] = c[0] / c[3]; sp.c[k][1] = c[1] / c[3]; sp.c[k][2] = c[2] / c[3];
         sp.c[k][3] = c[4] / c[3]; sp.c[k][4] = c[5] / c[3];
     }
-    // device address of the scratch, looked up once per device with that
-    // device current (the host-side symbol is only a stand-in)
+    // device address of the scratch, looked up once per device (and again
+    // if the device's context changed, e.g. after cudaDeviceReset) with that
+    // device current: the host-side symbol is only a stand-in
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return STFWI_ERR_CUDA;
+    void *ctx = nullptr;
+    ctx_current_fn cur = ctx_current();
+    if (cur) cur(&ctx);
     double *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            cudaError_t e = cudaGetSymbolAddress((void **)&g_noalloc_ptr[dev], g_noalloc_trace_sums);
+        NoallocSlot &slot = g_noalloc_slot[dev];
+        if (!slot.ptr || !ctx || slot.ctx != ctx) {
+            double *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_trace_sums);
             if (e != cudaSuccess) {
                 fprintf(stderr, "stfwi_misfit_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
-                g_noalloc_ptr[dev] = nullptr;
+                slot = NoallocSlot{};
                 return STFWI_ERR_CUDA;
             }
+            // the lookup made the primary context current if it was not yet
+            if (cur && !ctx) cur(&ctx);
+            slot.ctx = ctx;
+            slot.ptr = p;
         }
-        scratch = g_noalloc_ptr[dev];
+        scratch = slot.ptr;
     }
     Geo g{};
     g.nshot = nshot;
@@ -1691,7 +1595,7 @@ extern "C" stfwi_status stfwi_misfit_noalloc(int32_t nshot, int32_t nt, int32_t 
     g.nrec = nrec;
     cudaStream_t st = (cudaStream_t)stream;
     const int ntap = std::min(std::max(m->n_taper, 0), nt);
-    const int nnorm = m->reserved > 0 ? m->reserved : nshot;
+    const int nnorm = m->nshot_norm > 0 ? m->nshot_norm : nshot;
     const int n = nshot * nrec, thr = 128;
     k_misfit<<<(n + thr - 1) / thr, thr, 0, st>>>(g, m->component, ntap, sp, m->scale, nnorm, pred, obs, rec_adj,
                                                  scratch);

@@ -23,7 +23,9 @@ import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_reference_known_answers.py <path to the reference project>")
+ref = sys.argv[1]
 gc = np.load(os.path.join(ref, "Results_gradient/gradient_compare.npz"))
 gd = np.load(os.path.join(ref, "Results_gradient/gradient_data.npz"))
 fg = np.load(os.path.join(ref, "Results_first_gradient/first_gradient.npz"), allow_pickle=True)

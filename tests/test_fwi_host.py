@@ -67,18 +67,25 @@ def test_host_projection_matches_oracle_and_reference_rules():
 
 
 def test_driver_plateau_and_block_helpers():
-    """The stage helpers of fwi/optim_lbfgsb.py: plateau window, active
-    blocks, block scales."""
+    """The multiscale driver's stage helpers: the plateau window (the
+    reference's rule of fwi/optim_lbfgsb.py:117-134), the planes each
+    `invert` mode moves, per-plane scales and stage parsing."""
     from stfwi_b200.fwi import optim_lbfgsb as D
-    p = D._Plateau(3, 1e-3)
+    p = D.LossWindow(3, 1e-3)
     stops = [p.push(v) for v in (10, 9, 8, 7, 6, 5)]   # still dropping: no stop
     assert stops == [False] * 6
-    q = D._Plateau(3, 1e-3)
+    q = D.LossWindow(3, 1e-3)
     stops = [q.push(v) for v in (5.0, 5.0, 5.0, 5.0, 5.0, 4.999)]   # last 3 vs previous 3 within 0.1 %
     assert stops == [False] * 5 + [True]
-    assert D._Plateau(None, 1e-3).push(1.0) is False
-    assert D._active_keys("vs") == ["Vs"] and D._active_keys("all") == ["Vs", "Vp", "rho"]
+    assert D.LossWindow(None, 1e-3).push(1.0) is False
+    assert D.planes_of("vs") == (0,) and D.planes_of("all") == (0, 1, 2)
     with pytest.raises(ValueError):
-        D._active_keys("rho")
-    s = D._block_scales((np.array([[-3.0, 2.0]]), np.zeros((1, 2)), np.array([[1.0, 5.0]])))
-    assert s == [3.0, 1e-12, 5.0]
+        D.planes_of("rho")
+    s = D.plane_scales(np.stack([np.array([[-3.0, 2.0]]), np.zeros((1, 2)), np.array([[1.0, 5.0]])]))
+    assert s.tolist() == [3.0, 1e-12, 5.0]
+    spec = D.StageSpec.from_dict(dict(f_c=3.0, cutoff=2.0, n_iters=4))
+    assert (spec.invert, spec.precon, spec.n_taper_pct) == ("vs", "illum", 0.0)
+    with pytest.raises(ValueError):
+        D.StageSpec.from_dict(dict(f_c=3.0, precon="hessian"))
+    with pytest.raises(KeyError):
+        D.StageSpec.from_dict(dict(cutoff=3.0))

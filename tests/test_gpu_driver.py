@@ -143,18 +143,11 @@ def test_multiscale_driver_matches_oracle_driven_run(monkeypatch):
         a.pop("block_size", None)
         return O.compute_gradient("ad", d0_f32=True, **a)
 
-    class _Host:   # host array in place of a device tensor
-        def __init__(self, a):
-            self.a = a
-
-        def cpu(self):
-            return self
-
-        def numpy(self):
-            return self.a
-
-    def host_project(params, K_margin, vp_cap):
-        return [_Host(p) for p in O.project_velocity(*params, K_margin=K_margin, vp_cap=vp_cap)]
+    def host_project(self, model):   # the oracle's projection on the host, written back
+        import torch
+        p = O.project_velocity(*(a.cpu().numpy() for a in model), K_margin=self.K_margin, vp_cap=self.vp_cap)
+        model.copy_(torch.as_tensor(np.stack(p), device=model.device))
+        return model
 
     def oracle_illum(nz, nx, dx, dz, dt, nt_, f_c, pad, block_size, rec_x, rec_z, fd_order, component, Vs, Vp,
                      rho_, src_x, src_z, src_wavelet, eps):
@@ -166,7 +159,7 @@ def test_multiscale_driver_matches_oracle_driven_run(monkeypatch):
         return O.illumination_inverse(ws, nz, nx, pad, eps)
 
     monkeypatch.setattr(D, "compute_gradient", oracle_gradient)
-    monkeypatch.setattr(D, "_project", host_project)
+    monkeypatch.setattr(D.MultiscaleDriver, "_project", host_project)
     monkeypatch.setattr(D, "compute_illumination_for_stage", oracle_illum)
     _, h_ref = fwi.run_multiscale_fwi(**kw)
     for a, b in zip(h_gpu, h_ref):

@@ -2,12 +2,15 @@
 
 Some callers cannot call cudaMalloc: a custom call made from inside a
 framework that has reserved most of the device for its own memory pool (the
-JAX drivers of this workload preallocate 90 % of it), or code that records a
-stream capture.  stfwi_misfit_noalloc serves them with a fixed, file-scope
-device scratch array instead of a handle's workspace.  These tests call it
-through the C ABI and check it against the handle-based stfwi_misfit on the
-same traces, twice in a row (the scratch keeps the previous call's contents).
-This file is collected last on purpose.
+JAX drivers of this workload preallocate 90 % of it), where one more
+allocation can fail or fragment that pool.  stfwi_misfit_noalloc serves them
+with a fixed, file-scope device scratch array instead of a handle's
+workspace.  These tests call it through the C ABI and check it against the
+handle-based stfwi_misfit on the same traces, twice in a row (the scratch
+keeps the previous call's contents): once with a low-pass filter and the
+call's own shot count, once without a filter and with a larger shot count
+for the normalisation (a shard of a bigger batch).  This file is collected
+last on purpose.
 """
 import ctypes as ct
 
@@ -19,9 +22,11 @@ from tests import dot_case as C
 pytestmark = pytest.mark.gpu
 
 
-def _desc(N, component, scale, sos, n_taper):
+def _desc(N, component, scale, sos, n_taper, nshot_norm):
+    if sos is None:
+        return N.StfwiMisfitDesc(component, n_taper, 0, nshot_norm, scale, None), None
     sos_a = np.ascontiguousarray(np.asarray(sos, dtype=np.float64))
-    d = N.StfwiMisfitDesc(component, n_taper, sos_a.shape[0], 0, scale,
+    d = N.StfwiMisfitDesc(component, n_taper, sos_a.shape[0], nshot_norm, scale,
                           sos_a.ctypes.data_as(ct.POINTER(ct.c_double)))
     return d, sos_a
 
@@ -54,15 +59,15 @@ def test_noalloc_misfit_matches_handle_path_twice():
     comp, scale, n_taper = 1, 2.5, 12
     rng = np.random.default_rng(11)
     stream = ct.c_void_p(torch.cuda.current_stream().cuda_stream)
-    for call in range(2):
+    for call, (filt, nnorm) in enumerate(((sos, 0), (None, 7))):
         obs = torch.tensor(rng.standard_normal((3, nt, len(rx))) * 1e-9, dtype=torch.float32, device="cuda")
         # handle path
-        mis_ref = S.misfit(obs, comp, scale, sos, n_taper)
+        mis_ref = S.misfit(obs, comp, scale, filt, n_taper, nshot_norm=nnorm)
         src_ref = S.gradient(exact=False, src=True)["src"]
         # no-allocation path: device inputs and outputs owned by the caller
         rec_adj = torch.full((3, 4, nt, len(rx)), float("nan"), dtype=torch.float32, device="cuda")
         mis = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
-        d, sos_keep = _desc(N, comp, scale, sos, n_taper)
+        d, sos_keep = _desc(N, comp, scale, filt, n_taper, nnorm)
         st = lib.stfwi_misfit_noalloc(3, nt, len(rx), pred.data_ptr(), obs.data_ptr(), ct.byref(d),
                                       rec_adj.data_ptr(), mis.data_ptr(), stream)
         assert st == 0
