@@ -51,6 +51,60 @@ def build() -> str:
     return _LIB_PATH
 
 
+_FAST_PATH = os.path.join(_HERE, "liboracle_fast.so")
+_fast = None
+
+
+def build_fast() -> str:
+    """Compile liboracle_fast.so (FP32, -march=native, FP contraction, OpenMP
+    over shots) for THIS host: it is rebuilt on every call, as a copy made on
+    another machine may target another instruction set."""
+    subprocess.run(["make", "-s", "-B", "-C", _HERE, "fast"], check=True)
+    return _FAST_PATH
+
+
+def _bind(L, prefixes):
+    P = ct.POINTER
+    dp, ip = P(ct.c_double), P(ct.c_int32)
+    for pre in prefixes:
+        f = getattr(L, pre + "forward")
+        f.argtypes = [P(OracleDesc), dp, dp, dp, ct.c_int32, ct.c_int32, ct.c_int32, dp,
+                      ip, ip, dp, ct.c_int32, dp, ct.c_int32, dp]
+        f.restype = ct.c_int
+        f = getattr(L, pre + "adjoint")
+        f.argtypes = [P(OracleDesc), dp, dp, dp, ct.c_int32, ct.c_int32, ct.c_int32, dp,
+                      ip, ip, dp, dp, dp, dp, ct.c_int32, dp, ct.c_int32]
+        f.restype = ct.c_int
+        f = getattr(L, pre + "forward_batch")
+        f.argtypes = [P(OracleDesc), dp, dp, dp, ct.c_int32, ip, dp, ip, ip, dp]
+        f.restype = ct.c_int
+        f = getattr(L, pre + "gradient_batch")
+        f.argtypes = [P(OracleDesc), dp, dp, dp, ct.c_int32, ip, dp, ip, ip, dp, dp, dp,
+                      ct.c_int32]
+        f.restype = ct.c_int
+        f = getattr(L, pre + "pml_profiles")
+        f.argtypes = [P(OracleDesc), dp, dp]
+        f.restype = ct.c_int
+    return L
+
+
+def lib_fast():
+    """The tuned timing build (symbols oraclefast_*), built here on first use."""
+    global _fast
+    with _lock:
+        if _fast is None:
+            build_fast()
+            _fast = _bind(ct.CDLL(_FAST_PATH), ("oraclefast_",))
+        return _fast
+
+
+def _entry(name, precision):
+    """Entry point `name` of the FP64 (64), FP32 (32) or tuned FP32 ('fast') build."""
+    if precision == "fast":
+        return getattr(lib_fast(), "oraclefast_" + name)
+    return getattr(lib(), f"oracle{precision}_{name}")
+
+
 def lib():
     global _lib
     with _lock:
@@ -344,7 +398,7 @@ def forward_batch(Vs, Vp, rho, src_x, src_z, src_types, rec_x, rec_z, nx_dom, nz
                          [SRC_TYPES[t] for t in src_types]], axis=1))
     d = make_desc(nz_dom, nx_dom, pad, fd_order, free_surface, nt, rec_x.size, dx, dz, dt, fc, d0_f32)
     out = np.zeros((ns, 4, nt, rec_x.size))
-    fn = getattr(lib(), f"oracle{precision}_forward_batch")
+    fn = _entry("forward_batch", precision)
     rc = fn(ct.byref(d), _dptr(_f64(Vs)), _dptr(_f64(Vp)), _dptr(_f64(rho)), ns, _iptr(src),
             _dptr(_f64(src_wavelet)), _iptr(rec_x), _iptr(rec_z), _dptr(out))
     if rc:
@@ -368,7 +422,7 @@ def gradient_batch(Vs, Vp, rho, src_x, src_z, src_types, rec_x, rec_z, nx_dom, n
     nz, nx = grid_shape(nz_dom, nx_dom, pad, free_surface)
     gm = np.zeros((ns, 4, nz, nx)) if mode == "gmat" else None
     im = np.zeros((ns, 3, nz, nx)) if mode == "img" else None
-    fn = getattr(lib(), f"oracle{precision}_gradient_batch")
+    fn = _entry("gradient_batch", precision)
     rc = fn(ct.byref(d), _dptr(_f64(Vs)), _dptr(_f64(Vp)), _dptr(_f64(rho)), ns, _iptr(src),
             _dptr(_f64(src_wavelet)), _iptr(rec_x), _iptr(rec_z), _dptr(_f64(rec_adj)), _dptr(gm),
             _dptr(im), int(ckpt))

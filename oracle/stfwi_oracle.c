@@ -21,14 +21,23 @@
  *
  * Compiled twice: ORACLE_F32 undefined -> oracle64_* (FP64, the parity
  * oracle); ORACLE_F32 defined -> oracle32_* (FP32, the timed CPU baseline in
- * the reference's default dtype).  OpenMP parallelism is over shots.
+ * the reference's default dtype, every multiply and add rounded as written).
+ * OpenMP parallelism is over shots.  A third, tuned build (ORACLE_FAST ->
+ * oraclefast_*, liboracle_fast.so, made on the machine that times it) keeps
+ * the FP32 arithmetic but lets the compiler contract and vectorise for the
+ * host's own ISA.  (Splitting each slab's rows over threads was measured
+ * ten times slower: a slab is too small for a parallel region of its own.)
  */
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
-#ifdef ORACLE_F32
+#ifdef ORACLE_FAST
+/* the tuned timing build: FP32, native ISA, contraction allowed */
+typedef float real;
+#define ORACLE(n) oraclefast_##n
+#elif defined(ORACLE_F32)
 typedef float real;
 #define ORACLE(n) oracle32_##n
 #else
@@ -836,19 +845,30 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
     /* forward checkpoints (carry-in of steps 0, ckpt, 2*ckpt, ...) */
     const int nseg = (nt + ckpt - 1) / ckpt;
     real ***ck = NULL, ***seg = NULL, **inter = NULL, **tmp = NULL;
+    /* ckpt >= nt keeps every step of the first forward pass (one segment, no
+     * recompute of it); otherwise checkpoints and a recompute per segment */
+    const int store_all = need_fwd && nseg == 1;
     if (need_fwd) {
         ck = (real ***)malloc(sizeof(real **) * nseg);
-        real **C = carry_alloc(N);
-        for (int it = 0; it < nt; ++it) {
-            if (it % ckpt == 0) {
-                ck[it / ckpt] = carry_alloc(N);
-                for (int k = 0; k < NCARRY; ++k) memcpy(ck[it / ckpt][k], C[k], N * sizeof(real));
-            }
-            fwd_step(&g, C, (real)wavelet[it], NULL);
-        }
-        carry_free(C);
         seg = (real ***)malloc(sizeof(real **) * (ckpt + 1));
         for (int k = 0; k <= ckpt; ++k) seg[k] = carry_alloc(N);
+        if (store_all) {
+            ck[0] = NULL;
+            for (int it = 0; it < nt; ++it) {
+                for (int k = 0; k < NCARRY; ++k) memcpy(seg[it + 1][k], seg[it][k], N * sizeof(real));
+                fwd_step(&g, seg[it + 1], (real)wavelet[it], NULL);
+            }
+        } else {
+            real **C = carry_alloc(N);
+            for (int it = 0; it < nt; ++it) {
+                if (it % ckpt == 0) {
+                    ck[it / ckpt] = carry_alloc(N);
+                    for (int k = 0; k < NCARRY; ++k) memcpy(ck[it / ckpt][k], C[k], N * sizeof(real));
+                }
+                fwd_step(&g, C, (real)wavelet[it], NULL);
+            }
+            carry_free(C);
+        }
         inter = (real **)malloc(sizeof(real *) * NINTER);
         for (int k = 0; k < NINTER; ++k) inter[k] = zalloc(N);
         tmp = carry_alloc(N);
@@ -857,7 +877,7 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
     const int hmap[5] = {C_U, C_V, C_EX, C_EZ, C_ES};
     for (int s = nseg - 1; s >= 0; --s) {
         const int t0 = s * ckpt, t1 = (t0 + ckpt < nt) ? t0 + ckpt : nt;
-        if (need_fwd) {
+        if (need_fwd && !store_all) {
             /* seg[k] = carry-in of step t0+k, for k = 0 .. t1-t0 (last = carry-out of t1-1) */
             for (int k = 0; k < NCARRY; ++k) memcpy(seg[0][k], ck[s][k], N * sizeof(real));
             for (int it = t0; it < t1; ++it) {
@@ -916,7 +936,8 @@ int ORACLE(adjoint)(const oracle_desc *d, const double *vs, const double *vp, co
         for (size_t q = 0; q < N; ++q) { img[q] += glam[q]; img[N + q] += gmu[q]; img[2 * N + q] += grl[q]; }
 
     if (need_fwd) {
-        for (int k = 0; k < nseg; ++k) carry_free(ck[k]);
+        for (int k = 0; k < nseg; ++k)
+            if (ck[k]) carry_free(ck[k]);
         free(ck);
         for (int k = 0; k <= ckpt; ++k) carry_free(seg[k]);
         free(seg);
