@@ -24,6 +24,9 @@
  *   stfwi_gradient(STFWI_GRAD_IMAGING) the 'adjoint' backend's imaging,
  *                                    fwi/gradient.py:159-259, fwi/imaging.py:83-169
  *   stfwi_illumination               fwi/illumination.py:18-48 (Ws before cropping)
+ *   stfwi_forward_frames             forward_jax return_vars '*_full' / return_wavefields
+ *   stfwi_adjoint_frames             adjoint_jax(..., return_wavefields=True)
+ *   stfwi_imaging_condition          fwi/imaging.py:83-169 (imaging_condition)
  */
 #ifndef STFWI_H
 #define STFWI_H
@@ -220,6 +223,53 @@ stfwi_status stfwi_preconditioner(stfwi_handle *h, int32_t kind, int32_t compone
  * rho_floor.  No handle; host pointers return STFWI_ERR_INVALID. */
 stfwi_status stfwi_project_velocity(int64_t n, double *vs, double *vp, double *rho, double K_margin, double vp_cap,
                                     double vs_floor, double rho_floor, void *stream);
+
+/* Full wavefield frames (bit set; frames come out in bit order). */
+#define STFWI_FRAME_VX 1u  /* vx  (U)   forward; U_a adjoint */
+#define STFWI_FRAME_VZ 2u  /* vz  (V)   forward; V_a adjoint */
+#define STFWI_FRAME_EX 4u  /* exx       forward; ex_a adjoint */
+#define STFWI_FRAME_EZ 8u  /* ezz       forward; ez_a adjoint */
+#define STFWI_FRAME_ES 16u /* exz       forward; es_a adjoint */
+
+/* Forward modelling that also returns full wavefields: the reference's
+ * return_vars 'vx_full' .. 'es_full' and return_wavefields=True
+ * (fwi/forward.py:122,148-155,449-463).  frames = [nshot][nfields][nt][nz_t][nx_t]
+ * float32 (host or device), frame n = the state after step n, strains
+ * recovered from the carried stresses.  The receiver traces are filled as by
+ * stfwi_forward; no strain history is kept.  A device staging buffer of
+ * nshot * nfields padded grids is allocated for the call (STFWI_ERR_OOM if it
+ * does not fit). */
+stfwi_status stfwi_forward_frames(stfwi_handle *h, uint32_t fields, float *frames, void *stream);
+
+/* Adjoint sweep of the source-wavelet adjoint (STFWI_GRAD_SRC) that also
+ * returns the adjoint wavefields: adjoint_jax(..., return_wavefields=True)
+ * (fwi/adjoint_jax_kernel.py:69,91-93,470-483).  frames = [nshot][nfields]
+ * [nt][nz_t][nx_t] float32 (host or device) of (U_a, V_a, ex_a, ez_a, es_a)
+ * by STFWI_FRAME_* bits, in forward-time order: frame n = the carry out of
+ * adjoint step n.  src_wav_a = [nshot][nt].  Adjoint sources come from
+ * stfwi_set_adjoint_sources or stfwi_misfit. */
+stfwi_status stfwi_adjoint_frames(stfwi_handle *h, uint32_t fields, float *frames, float *src_wav_a,
+                                  void *stream);
+
+/* The reference's imaging condition on histories the caller holds
+ * (fwi/imaging.py:83-169 imaging_condition), without a handle. */
+typedef struct {
+    int32_t nz_dom, nx_dom, pad, free_surface, nt;
+    int32_t time_chunk; /* frames per chunk of the time sums (0: 64) */
+    double dx, dz, dt;
+} stfwi_imaging_desc;
+
+/* vs, vp, rho: [nz_dom][nx_dom] float32; ex, ez, es, ua, va (and optionally
+ * vx, vz, both or neither): [nt][nz_t][nx_t] float32 histories of the forward
+ * strains, adjoint velocities and forward velocities, host or device memory
+ * (host histories are copied a chunk at a time).  g_out = [6][nz_dom][nx_dom]
+ * FP64 (host or device): g_Vs, g_Vp, g_rho, g_lam, g_mu, g_rho_lame.  Time
+ * sums in FP64.  Allocates its working buffers for the call; errors are
+ * printed to stderr. */
+stfwi_status stfwi_imaging_condition(const stfwi_imaging_desc *d, const float *vs, const float *vp,
+                                     const float *rho, const float *ex_hist, const float *ez_hist,
+                                     const float *es_hist, const float *ua_hist, const float *va_hist,
+                                     const float *vx_hist, const float *vz_hist, double *g_out, void *stream);
 
 /* Padded-grid shape of a descriptor. */
 void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t);

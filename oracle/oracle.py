@@ -544,3 +544,41 @@ def eprecond3_multiplier(Ws_padded, rec_x, rec_z, dx, dz, free_surface, pad, nz_
     We = We + eps * np.max(We)
     p = 1.0 / We[z0:z0 + nz_dom, pad:pad + nx_dom]
     return p / np.max(p)
+
+
+def imaging_condition(Vs, Vp, rho, ex_hist, ez_hist, es_hist, U_a_hist, V_a_hist, dx, dz, dt, pad,
+                      free_surface, nz_dom, nx_dom, vx_hist=None, vz_hist=None):
+    """fwi/imaging.py:83-169 in NumPy FP64 on full histories (nt, nz_t, nx_t):
+    B of the nearest-neighbour extension of rho (:56-80, :113-114), periodic
+    centred differences of B U_a and B V_a (np.roll, :47-53), the Lame sums
+    (:125-141), the density term with the centred time derivative (:145-154),
+    the crop and the chain rule (:157-167).  Returns (g_Vs, g_Vp, g_rho,
+    g_lam, g_mu, g_rho_lame)."""
+    z0 = 0 if free_surface else pad
+    nz, nx = grid_shape(nz_dom, nx_dom, pad, free_surface)
+    ii = np.clip(np.arange(nz) - z0, 0, nz_dom - 1)
+    jj = np.clip(np.arange(nx) - pad, 0, nx_dom - 1)
+    B = 1.0 / np.asarray(rho, dtype=np.float64)[np.ix_(ii, jj)]
+    ua, va = np.asarray(U_a_hist, np.float64), np.asarray(V_a_hist, np.float64)
+    BU, BV = B * ua, B * va
+
+    def cd(f, h, ax):
+        return (np.roll(f, -1, axis=ax) - np.roll(f, 1, axis=ax)) / (2.0 * h)
+
+    dxBU, dzBV, dzBU, dxBV = cd(BU, dx, 2), cd(BV, dz, 1), cd(BU, dz, 1), cd(BV, dx, 2)
+    ex, ez, es = (np.asarray(a, np.float64) for a in (ex_hist, ez_hist, es_hist))
+    g_lam = -dt * np.sum((ex + ez) * (dxBU + dzBV), axis=0)
+    g_mu = -dt * np.sum(2.0 * ex * dxBU + 2.0 * ez * dzBV + es * (dzBU + dxBV), axis=0)
+    g_rl = np.zeros((nz, nx))
+    if vx_hist is not None:
+        vx, vz = np.asarray(vx_hist, np.float64), np.asarray(vz_hist, np.float64)
+        dua = (ua[2:] - ua[:-2]) / (2.0 * dt)
+        dva = (va[2:] - va[:-2]) / (2.0 * dt)
+        g_rl = -dt * np.sum(vx[1:-1] * dua + vz[1:-1] * dva, axis=0)
+    sl = (slice(z0, z0 + nz_dom), slice(pad, pad + nx_dom))
+    g_lam, g_mu, g_rl = g_lam[sl], g_mu[sl], g_rl[sl]
+    Vs, Vp, r = (np.asarray(a, np.float64) for a in (Vs, Vp, rho))
+    g_Vs = 2.0 * r * Vs * (g_mu - 2.0 * g_lam)
+    g_Vp = 2.0 * r * Vp * g_lam
+    g_rho = (Vp ** 2 - 2.0 * Vs ** 2) * g_lam + Vs ** 2 * g_mu + g_rl
+    return g_Vs, g_Vp, g_rho, g_lam, g_mu, g_rl

@@ -27,7 +27,11 @@ EXPORTS = (
     "stfwi_set_adjoint_sources", "stfwi_gradient", "stfwi_illumination", "stfwi_check",
     "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
     "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
+    "stfwi_forward_frames", "stfwi_adjoint_frames", "stfwi_imaging_condition",
 )
+
+# full wavefield frames (bit set, in this order)
+FRAME_BITS = {"vx": 1, "vz": 2, "ex": 4, "ez": 8, "es": 16}
 
 # every symbol include/stfwi_nn.h declares (the learned preconditioner's network kernels)
 NN_EXPORTS = (
@@ -57,6 +61,14 @@ class StfwiMisfitDesc(ct.Structure):
     _fields_ = [
         ("component", ct.c_int32), ("n_taper", ct.c_int32), ("nsos", ct.c_int32),
         ("nshot_norm", ct.c_int32), ("scale", ct.c_double), ("sos", ct.POINTER(ct.c_double)),
+    ]
+
+
+class StfwiImagingDesc(ct.Structure):
+    _fields_ = [
+        ("nz_dom", ct.c_int32), ("nx_dom", ct.c_int32), ("pad", ct.c_int32), ("free_surface", ct.c_int32),
+        ("nt", ct.c_int32), ("time_chunk", ct.c_int32),
+        ("dx", ct.c_double), ("dz", ct.c_double), ("dt", ct.c_double),
     ]
 
 
@@ -105,6 +117,9 @@ def load():
         L.stfwi_preconditioner.argtypes = [H, i32, i32, f64, vp, vp]
         L.stfwi_project_velocity.argtypes = [ct.c_int64, vp, vp, vp, f64, f64, f64, f64, vp]
         L.stfwi_autotune.argtypes = [H, i32, vp, vp]
+        L.stfwi_forward_frames.argtypes = [H, u32, vp, vp]
+        L.stfwi_adjoint_frames.argtypes = [H, u32, vp, vp, vp]
+        L.stfwi_imaging_condition.argtypes = [ct.POINTER(StfwiImagingDesc)] + [vp] * 10 + [vp, vp]
         sz, f32 = ct.c_size_t, ct.c_float
         L.stfwi_nn_last_error.argtypes = []
         L.stfwi_nn_last_error.restype = ct.c_char_p

@@ -751,6 +751,159 @@ void set_groups(stfwi_handle *h, const int spg_in[4])
 
 // ================================================================ C ABI
 
+
+// ---------------------------------------------------------------- full wavefield frames
+
+namespace {
+
+// frame of the forward state of every shot after a step: U, V and the
+// strains recovered from the carried stresses, on the padded grid (no pitch)
+__global__ void k_frames_fwd(Geo g, Mat m, const float *F, uint32_t fields, int nf, float *out)
+{
+    const long long N = (long long)g.nz * g.nx;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (q >= N) return;
+    const int i = (int)(q / g.nx), j = (int)(q % g.nx);
+    const long long o = (long long)i * g.P + j;
+    const float *f = F + (long long)s * F_N * g.fstride;
+    float v[5];
+    v[0] = f[F_U * g.fstride + o];
+    v[1] = f[F_V * g.fstride + o];
+    strains_of(f[F_EX * g.fstride + o], f[F_EZ * g.fstride + o], f[F_ES * g.fstride + o], m.L2M[o], m.L[o],
+               m.M[o], v[2], v[3], v[4]);
+    int k = 0;
+#pragma unroll
+    for (int b = 0; b < 5; ++b)
+        if (fields >> b & 1u) out[((long long)s * nf + k++) * N + q] = v[b];
+}
+
+// frame of the adjoint state after adjoint step n: U_a = P / B, V_a = Q / B
+// and the three strain adjoints
+__global__ void k_frames_adj(Geo g, Mat m, const float *A, uint32_t fields, int nf, float *out)
+{
+    const long long N = (long long)g.nz * g.nx;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (q >= N) return;
+    const int i = (int)(q / g.nx), j = (int)(q % g.nx);
+    const long long o = (long long)i * g.P + j;
+    const float *a = A + (long long)s * F_N * g.fstride;
+    const float b = m.B[o];
+    const float v[5] = {a[F_U * g.fstride + o] / b, a[F_V * g.fstride + o] / b, a[F_EX * g.fstride + o],
+                        a[F_EZ * g.fstride + o], a[F_ES * g.fstride + o]};
+    int k = 0;
+#pragma unroll
+    for (int b2 = 0; b2 < 5; ++b2)
+        if (fields >> b2 & 1u) out[((long long)s * nf + k++) * N + q] = v[b2];
+}
+
+// the strain-phase kernel of adjoint step n already added the exx / ezz
+// receiver sources of step n - 1 (the start of the next adjoint step): take
+// them out of the frame of step n
+__global__ void k_frames_unpick(Geo g, const int *rx, const int *rz, const float *rec_adj, int n, int kex,
+                                int kez, int nf, float *out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nshot * g.nrec || n < 1) return;
+    const int s = t / g.nrec, r = t % g.nrec;
+    const long long N = (long long)g.nz * g.nx, q = (long long)rz[r] * g.nx + rx[r];
+    const float *src = rec_adj + (long long)s * 4 * g.nt * g.nrec + (long long)(n - 1) * g.nrec + r;
+    if (kex >= 0) atomicAdd(out + ((long long)s * nf + kex) * N + q, -src[2LL * g.nt * g.nrec]);
+    if (kez >= 0) atomicAdd(out + ((long long)s * nf + kez) * N + q, -src[3LL * g.nt * g.nrec]);
+}
+
+// fwi/imaging.py:83-169 on histories held by the caller: one thread per
+// physical cell sums, over the frames [t0, t1) of a chunk, the Lame terms
+// with the periodic centred differences of B U_a and B V_a (jnp.roll wraps
+// across the padded grid) and, with the forward velocities, the density
+// term with the centred time derivative of the adjoint velocities.  The
+// chunk arrays hold frames [c0, c0 + ...) (ua, va from c0 - 1 when t0 > 0).
+struct ImgArgs {
+    int nz, nx, nz_dom, nx_dom, z0, pad, nt;
+    double dt, inv2dx, inv2dz;
+    const float *rho;                       // physical [nz_dom][nx_dom]
+    const float *ex, *ez, *es, *vx, *vz;    // frames t0.. of the chunk
+    const float *ua, *va;                   // frames ua0.. (one before t0 when t0 > 0)
+    int t0, t1, ua0;
+    double *acc;                            // [3][nd]: g_lam, g_mu, g_rho_lame
+};
+
+__device__ __forceinline__ double b_ext(const ImgArgs &a, int i, int j)
+{
+    // buoyancy of the nearest-neighbour extension of rho (fwi/imaging.py:56-80)
+    const int pi = min(max(i - a.z0, 0), a.nz_dom - 1), pj = min(max(j - a.pad, 0), a.nx_dom - 1);
+    return 1.0 / (double)a.rho[(long long)pi * a.nx_dom + pj];
+}
+
+__global__ void k_imaging_hist(ImgArgs a)
+{
+    const long long nd = (long long)a.nz_dom * a.nx_dom;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= nd) return;
+    const int i = (int)(q / a.nx_dom) + a.z0, j = (int)(q % a.nx_dom) + a.pad;
+    const long long N = (long long)a.nz * a.nx;
+    const int ip = (i + 1) % a.nz, im = (i - 1 + a.nz) % a.nz, jp = (j + 1) % a.nx, jm = (j - 1 + a.nx) % a.nx;
+    const long long o = (long long)i * a.nx + j;
+    const long long oxp = (long long)i * a.nx + jp, oxm = (long long)i * a.nx + jm;
+    const long long ozp = (long long)ip * a.nx + j, ozm = (long long)im * a.nx + j;
+    const double bxp = b_ext(a, i, jp), bxm = b_ext(a, i, jm), bzp = b_ext(a, ip, j), bzm = b_ext(a, im, j);
+    double glam = 0.0, gmu = 0.0, grl = 0.0;
+    for (int t = a.t0; t < a.t1; ++t) {
+        const float *u = a.ua + (long long)(t - a.ua0) * N, *v = a.va + (long long)(t - a.ua0) * N;
+        const long long f = (long long)(t - a.t0) * N;
+        const double dxBU = (bxp * u[oxp] - bxm * u[oxm]) * a.inv2dx;
+        const double dzBU = (bzp * u[ozp] - bzm * u[ozm]) * a.inv2dz;
+        const double dxBV = (bxp * v[oxp] - bxm * v[oxm]) * a.inv2dx;
+        const double dzBV = (bzp * v[ozp] - bzm * v[ozm]) * a.inv2dz;
+        const double e1 = a.ex[f + o], e2 = a.ez[f + o], e3 = a.es[f + o];
+        glam -= a.dt * ((e1 + e2) * (dxBU + dzBV));
+        gmu -= a.dt * (2.0 * e1 * dxBU + 2.0 * e2 * dzBV + e3 * (dzBU + dxBV));
+        if (a.vx && t >= 1 && t <= a.nt - 2) {
+            const double dua = ((double)u[N + o] - (double)u[o - N]) / (2.0 * a.dt);
+            const double dva = ((double)v[N + o] - (double)v[o - N]) / (2.0 * a.dt);
+            grl -= a.dt * ((double)a.vx[f + o] * dua + (double)a.vz[f + o] * dva);
+        }
+    }
+    a.acc[q] += glam;
+    a.acc[nd + q] += gmu;
+    a.acc[2 * nd + q] += grl;
+}
+
+// chain rule to (Vs, Vp, rho) after the crop (fwi/imaging.py:165-167)
+__global__ void k_imaging_chain(long long nd, const float *vs, const float *vp, const float *rho, const double *acc,
+                                double *g)
+{
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= nd) return;
+    const double Vs = vs[q], Vp = vp[q], r = rho[q], gl = acc[q], gm = acc[nd + q], grl = acc[2 * nd + q];
+    g[q] = 2.0 * r * Vs * (gm - 2.0 * gl);
+    g[nd + q] = 2.0 * r * Vp * gl;
+    g[2 * nd + q] = (Vp * Vp - 2.0 * Vs * Vs) * gl + Vs * Vs * gm + grl;
+    g[3 * nd + q] = gl;
+    g[4 * nd + q] = gm;
+    g[5 * nd + q] = grl;
+}
+
+bool device_resident(const void *p)
+{
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int popc5(uint32_t f)
+{
+    int n = 0;
+    for (int b = 0; b < 5; ++b) n += (f >> b) & 1u;
+    return n;
+}
+
+}  // namespace
+
 extern "C" {
 
 void stfwi_grid_shape(const stfwi_desc *d, int32_t *nz_t, int32_t *nx_t)
@@ -1490,6 +1643,196 @@ stfwi_status stfwi_check(stfwi_handle *h, void *stream)
     CK(h, cudaStreamSynchronize((cudaStream_t)stream));
     if (v & 1) return fail(h, STFWI_ERR_NONFINITE, "a receiver sample became non-finite (unstable dt or model?)");
     if (v & ST_TIMEOUT3) return fail(h, STFWI_ERR_TIMEOUT, "a tile copy did not complete within the wait limit");
+    return STFWI_OK;
+}
+
+
+stfwi_status stfwi_forward_frames(stfwi_handle *h, uint32_t fields, float *frames, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if (!frames || fields == 0 || fields >= 32u) return fail(h, STFWI_ERR_INVALID, "no frames or bad field mask");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    const int nf = popc5(fields);
+    const size_t N = (size_t)g.nz * g.nx, sbytes = (size_t)h->nshot * nf * N * sizeof(float);
+    float *stage = nullptr;
+    if (cudaMallocAsync((void **)&stage, sbytes, st) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, STFWI_ERR_OOM, "no room for the %zu-byte frame staging buffer", sbytes);
+    }
+    rc = zero_forward_state(h, st);
+    if (rc) { cudaFreeAsync(stage, st); return rc; }
+    FwdOut o{};
+    o.rec = h->rec;
+    o.status = h->status;
+    o.slots = h->slots;
+    const dim3 grid((unsigned)((N + 255) / 256), h->nshot);
+    for (int n = 0; n < g.nt; ++n) {
+        fwd_step(h, n, o, st);
+        k_frames_fwd<<<grid, 256, 0, st>>>(g, mat_of(h), h->F, fields, nf, stage);
+        // frame n of every (shot, field) plane: rows of N floats, nt frames apart
+        cudaError_t e = cudaMemcpy2DAsync(frames + (size_t)n * N, (size_t)g.nt * N * sizeof(float), stage,
+                                          N * sizeof(float), N * sizeof(float), (size_t)h->nshot * nf,
+                                          cudaMemcpyDefault, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(stage, st);
+            return fail(h, STFWI_ERR_CUDA, "frame copy: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaFreeAsync(stage, st);
+    h->stored = false;
+    CK(h, cudaGetLastError());
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_adjoint_frames(stfwi_handle *h, uint32_t fields, float *frames, float *src_wav_a, void *stream)
+{
+    stfwi_status rc = ready(h);
+    if (rc) return rc;
+    if (!frames || fields == 0 || fields >= 32u) return fail(h, STFWI_ERR_INVALID, "no frames or bad field mask");
+    if (!src_wav_a) return fail(h, STFWI_ERR_INVALID, "src_wav_a is null");
+    cudaStream_t st = (cudaStream_t)stream;
+    const Geo &g = h->g;
+    const int nf = popc5(fields);
+    int kex = -1, kez = -1;
+    for (int b = 0, k = 0; b < 5; ++b)
+        if (fields >> b & 1u) {
+            if (b == 2) kex = k;
+            if (b == 3) kez = k;
+            ++k;
+        }
+    const size_t N = (size_t)g.nz * g.nx, sbytes = (size_t)h->nshot * nf * N * sizeof(float);
+    float *stage = nullptr;
+    if (cudaMallocAsync((void **)&stage, sbytes, st) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, STFWI_ERR_OOM, "no room for the %zu-byte frame staging buffer", sbytes);
+    }
+    rc = zero_adjoint_state(h, st);
+    if (rc) { cudaFreeAsync(stage, st); return rc; }
+    const int thr = 256;
+    const unsigned nrb = (unsigned)((g.nshot * std::max(g.nrec, 1) + thr - 1) / thr);
+    if (g.nrec > 0) k_inject_last<<<nrb, thr, 0, st>>>(g, h->rx, h->rz, h->rec_adj, h->A);
+    const dim3 grid((unsigned)((N + 255) / 256), h->nshot);
+    for (int n = g.nt - 1; n >= 0; --n) {
+        const int ping = (g.nt - 1 - n) & 1;
+        AdjIn ai{};
+        ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = 0;
+        ai.accLr = h->accLr; ai.want_exact = 0; ai.ping = ping;
+        AdjOut ao{};
+        ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = -1; ao.slot_img = -1; ao.slot_next = -1;
+        ao.accp = h->accp; ao.acc = h->acc; ao.src_a = h->src_a; ao.rec_adj = h->rec_adj; ao.ping = ping;
+        switch (h->d.fd_order) {
+        case 2: launch_adj_step<2>(h, n, ai, ao, st); break;
+        case 4: launch_adj_step<4>(h, n, ai, ao, st); break;
+        default: launch_adj_step<8>(h, n, ai, ao, st); break;
+        }
+        k_frames_adj<<<grid, 256, 0, st>>>(g, mat_of(h), h->A, fields, nf, stage);
+        if (g.nrec > 0 && n > 0 && (kex >= 0 || kez >= 0))
+            k_frames_unpick<<<nrb, thr, 0, st>>>(g, h->rx, h->rz, h->rec_adj, n, kex, kez, nf, stage);
+        cudaError_t e = cudaMemcpy2DAsync(frames + (size_t)n * N, (size_t)g.nt * N * sizeof(float), stage,
+                                          N * sizeof(float), N * sizeof(float), (size_t)h->nshot * nf,
+                                          cudaMemcpyDefault, st);
+        if (e != cudaSuccess) {
+            cudaFreeAsync(stage, st);
+            return fail(h, STFWI_ERR_CUDA, "frame copy: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaFreeAsync(stage, st);
+    CK(h, cudaGetLastError());
+    CK(h, cudaMemcpyAsync(src_wav_a, h->src_a, (size_t)h->nshot * g.nt * 4, cudaMemcpyDefault, st));
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_imaging_condition(const stfwi_imaging_desc *d, const float *vs, const float *vp, const float *rho,
+                                     const float *ex_hist, const float *ez_hist, const float *es_hist,
+                                     const float *ua_hist, const float *va_hist, const float *vx_hist,
+                                     const float *vz_hist, double *g_out, void *stream)
+{
+    if (!d || !vs || !vp || !rho || !ex_hist || !ez_hist || !es_hist || !ua_hist || !va_hist || !g_out) {
+        fprintf(stderr, "stfwi_imaging_condition: null argument\n");
+        return STFWI_ERR_INVALID;
+    }
+    if ((vx_hist == nullptr) != (vz_hist == nullptr)) {
+        fprintf(stderr, "stfwi_imaging_condition: give both forward velocity histories or neither\n");
+        return STFWI_ERR_INVALID;
+    }
+    if (d->nz_dom < 1 || d->nx_dom < 1 || d->pad < 0 || d->nt < 1 || !(d->dx > 0) || !(d->dz > 0) || !(d->dt > 0)) {
+        fprintf(stderr, "stfwi_imaging_condition: bad descriptor\n");
+        return STFWI_ERR_INVALID;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nz = d->free_surface ? d->nz_dom + d->pad : d->nz_dom + 2 * d->pad, nx = d->nx_dom + 2 * d->pad;
+    const long long N = (long long)nz * nx, nd = (long long)d->nz_dom * d->nx_dom;
+    const int C = d->time_chunk > 0 ? d->time_chunk : 64;
+    const bool rho_term = vx_hist != nullptr;
+    // device copies of what is not device memory: the model, and chunks of
+    // the histories (adjoint velocities with one frame on either side)
+    const float *hist[7] = {ex_hist, ez_hist, es_hist, vx_hist, vz_hist, ua_hist, va_hist};
+    bool dev[7];
+    size_t stage_floats = 0;
+    for (int k = 0; k < 7; ++k) {
+        dev[k] = hist[k] ? device_resident(hist[k]) : true;
+        if (!dev[k]) stage_floats += (size_t)(C + 2) * N;
+    }
+    const size_t model_floats = 3 * (size_t)nd;
+    float *buf = nullptr;
+    double *acc = nullptr, *gdev = nullptr;
+    auto bail = [&](const char *what, cudaError_t e) {
+        fprintf(stderr, "stfwi_imaging_condition: %s: %s\n", what, cudaGetErrorString(e));
+        cudaGetLastError();
+        if (buf) cudaFreeAsync(buf, st);
+        if (acc) cudaFreeAsync(acc, st);
+        if (gdev) cudaFreeAsync(gdev, st);
+        return e == cudaErrorMemoryAllocation ? STFWI_ERR_OOM : STFWI_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaMallocAsync((void **)&buf, (stage_floats + model_floats) * sizeof(float), st)) != cudaSuccess)
+        return bail("staging", e);
+    if ((e = cudaMallocAsync((void **)&acc, 3 * nd * sizeof(double), st)) != cudaSuccess) return bail("sums", e);
+    if ((e = cudaMallocAsync((void **)&gdev, 6 * nd * sizeof(double), st)) != cudaSuccess) return bail("output", e);
+    if ((e = cudaMemsetAsync(acc, 0, 3 * nd * sizeof(double), st)) != cudaSuccess) return bail("memset", e);
+    float *mvs = buf + stage_floats, *mvp = mvs + nd, *mrho = mvp + nd;
+    if ((e = cudaMemcpyAsync(mvs, vs, nd * 4, cudaMemcpyDefault, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(mvp, vp, nd * 4, cudaMemcpyDefault, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(mrho, rho, nd * 4, cudaMemcpyDefault, st)) != cudaSuccess)
+        return bail("model copy", e);
+    float *stage[7] = {nullptr};
+    for (int k = 0, off = 0; k < 7; ++k)
+        if (!dev[k]) { stage[k] = buf + (size_t)off * (C + 2) * N; ++off; }
+    ImgArgs a{};
+    a.nz = nz; a.nx = nx; a.nz_dom = d->nz_dom; a.nx_dom = d->nx_dom; a.z0 = d->free_surface ? 0 : d->pad;
+    a.pad = d->pad; a.nt = d->nt; a.dt = d->dt; a.inv2dx = 1.0 / (2.0 * d->dx); a.inv2dz = 1.0 / (2.0 * d->dz);
+    a.rho = mrho; a.acc = acc;
+    for (int t0 = 0; t0 < d->nt; t0 += C) {
+        const int t1 = std::min(t0 + C, d->nt);
+        const int u0 = std::max(t0 - 1, 0), u1 = std::min(t1 + 1, d->nt);   // adjoint frames [u0, u1)
+        const float *ptr[7];
+        for (int k = 0; k < 7; ++k) {
+            if (!hist[k]) { ptr[k] = nullptr; continue; }
+            const int f0 = k >= 5 ? u0 : t0, f1 = k >= 5 ? u1 : t1;
+            if (dev[k]) {
+                ptr[k] = hist[k] + (size_t)f0 * N;
+            } else {
+                if ((e = cudaMemcpyAsync(stage[k], hist[k] + (size_t)f0 * N, (size_t)(f1 - f0) * N * 4,
+                                         cudaMemcpyDefault, st)) != cudaSuccess)
+                    return bail("history copy", e);
+                ptr[k] = stage[k];
+            }
+        }
+        a.ex = ptr[0]; a.ez = ptr[1]; a.es = ptr[2];
+        a.vx = rho_term ? ptr[3] : nullptr; a.vz = rho_term ? ptr[4] : nullptr;
+        a.ua = ptr[5]; a.va = ptr[6];
+        a.t0 = t0; a.t1 = t1; a.ua0 = u0;
+        k_imaging_hist<<<(unsigned)((nd + 127) / 128), 128, 0, st>>>(a);
+    }
+    k_imaging_chain<<<(unsigned)((nd + 255) / 256), 256, 0, st>>>(nd, mvs, mvp, mrho, acc, gdev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return bail("launch", e);
+    if ((e = cudaMemcpyAsync(g_out, gdev, 6 * nd * sizeof(double), cudaMemcpyDefault, st)) != cudaSuccess)
+        return bail("output copy", e);
+    cudaFreeAsync(buf, st);
+    cudaFreeAsync(acc, st);
+    cudaFreeAsync(gdev, st);
     return STFWI_OK;
 }
 

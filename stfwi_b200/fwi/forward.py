@@ -1,5 +1,9 @@
 """Forward modelling with the reference's signatures (fwi/forward.py).
 
+Full wavefields ('vx_full' .. 'es_full', ``return_wavefields``) come from
+stfwi_forward_frames: the state of every step copied out of the GPU into a
+page-locked host array (nt x nz_t x nx_t float32 per field and shot).
+
 ``build_forward_fn(...)`` returns ``run_shot(Vs, Vp, rho, src_x, src_z,
 src_wavelet)`` as the reference does (fwi/forward.py:508-544), backed by one
 GPU handle per geometry; ``run_shot.batch`` runs many shots in one launch
@@ -12,6 +16,7 @@ import numpy as np
 from ..solver import Solver
 
 _REC = {"vx": 0, "vz": 1, "ex": 2, "ez": 3}
+_FULL = ("vx_full", "vz_full", "ex_full", "ez_full", "es_full")
 
 
 def ricker_jax(t, fc, t0, scaling_factor=1):
@@ -24,12 +29,7 @@ def _check_vars(return_vars):
     if return_vars is None:
         return ("vx", "vz", "ex", "ez")
     for k in return_vars:
-        if k.endswith("_full"):
-            raise NotImplementedError(
-                f"return_vars {k!r}: full wavefield histories are not materialised; use "
-                "compute_illumination_for_stage for sum_t field**2 and compute_gradient(backend="
-                "'cuda_imaging') for the imaging condition, both fused on the GPU")
-        if k not in _REC:
+        if k not in _REC and k not in _FULL:
             raise ValueError(f"unknown return var {k!r}")
     return tuple(return_vars)
 
@@ -67,9 +67,14 @@ class _ShotRunner:
         S = self.solver(sx.size)
         S.set_model(Vs, Vp, rho)
         S.set_shots(sx, sz, src_type or self.src_type, np.asarray(src_wavelet, dtype=np.float32))
-        S.forward()
+        full = [k[:-5] for k in self.vars if k in _FULL]
+        if full:
+            # full wavefields (fwi/forward.py:449-463): frames after every step
+            frames, _ = S.forward_frames(full)
+        else:
+            S.forward()
         rec = S.records()
-        return tuple(rec[:, _REC[k]] for k in self.vars)
+        return tuple(frames[k[:-5]] if k in _FULL else rec[:, _REC[k]] for k in self.vars)
 
     def __call__(self, Vs, Vp, rho, src_x, src_z, src_wavelet):
         out = self.batch(Vs, Vp, rho, [int(src_x)], [int(src_z)], src_wavelet)
@@ -90,13 +95,16 @@ def forward_jax(Vs, Vp, rho, src_x, src_z, rec_x, rec_z, nx_dom, nz_dom, dx, dz,
                 src_wavelet, return_wavefields=False, block_size=100, return_vars=None, fd_order=2,
                 free_surface=True, src_type="force"):
     """One shot of fwi/forward.py:119-501 on the GPU; returns
-    (rec_vx, rec_vz, rec_exx, rec_ezz) or the requested ``return_vars``."""
+    (rec_vx, rec_vz, rec_exx, rec_ezz), with ``return_wavefields`` followed
+    by the (nt, nz_t, nx_t) frames of U, V, exx, ezz, or the requested
+    ``return_vars`` (receiver names and '*_full' frames)."""
     if fd_order not in (2, 4, 8):
         raise NotImplementedError(f"fd_order={fd_order} not supported (use 2, 4, or 8).")
     if src_type not in ("force", "moment"):
         raise NotImplementedError(f"src_type={src_type!r} not supported (use 'force' or 'moment').")
     if return_wavefields and return_vars is None:
-        raise NotImplementedError("return_wavefields: full wavefield histories are not materialised")
+        # fwi/forward.py:460-461: the receiver tuple, then the U, V, ex, ez frames
+        return_vars = ["vx", "vz", "ex", "ez", "vx_full", "vz_full", "ex_full", "ez_full"]
     run = _ShotRunner(nz_dom, nx_dom, dx, dz, dt, nt, fc, pad, rec_x, rec_z, fd_order, free_surface,
                       return_vars, src_type)
     try:

@@ -227,6 +227,56 @@ class Solver:
             out["src"] = sa
         return out
 
+    def _frames_buffer(self, nf):
+        """Host buffer for [nshot, nf, nt, nz_t, nx_t] float32 frames: page-locked
+        when torch can provide it (the per-step copies then run asynchronously)."""
+        shape = (self.nshot, nf, self.nt, self.nz, self.nx)
+        t = _torch()
+        if t is not None and t.cuda.is_available():
+            try:
+                buf = t.empty(shape, dtype=t.float32, pin_memory=True)
+                return buf.numpy(), buf
+            except RuntimeError:
+                pass
+        a = np.empty(shape, dtype=np.float32)
+        return a, a
+
+    @staticmethod
+    def _field_mask(fields):
+        mask = 0
+        for f in fields:
+            if f not in N.FRAME_BITS:
+                raise ValueError(f"unknown field {f!r}; use {sorted(N.FRAME_BITS)}")
+            mask |= N.FRAME_BITS[f]
+        return mask
+
+    def forward_frames(self, fields=("vx", "vz", "ex", "ez", "es"), out=None):
+        """Forward run that also returns full padded-grid wavefields: a dict
+        field -> [nshot, nt, nz_t, nx_t] float32 (frame n = after step n), in
+        the order of ``fields`` ('vx', 'vz', 'ex', 'ez', 'es').  The receiver
+        traces of the run are available from ``records()`` as usual."""
+        mask = self._field_mask(fields)
+        order = [f for f in N.FRAME_BITS if mask & N.FRAME_BITS[f]]
+        arr, keep = (out, out) if out is not None else self._frames_buffer(len(order))
+        ptr = arr.ctypes.data if isinstance(arr, np.ndarray) else arr.data_ptr()
+        self._ok(self.lib.stfwi_forward_frames(self.h, mask, ptr, _stream()), "forward_frames")
+        self.check()
+        return {f: arr[:, order.index(f)] for f in fields}, keep
+
+    def adjoint_frames(self, fields=("vx", "vz", "ex", "ez", "es"), out=None):
+        """Source-wavelet adjoint sweep that also returns the adjoint
+        wavefields (U_a, V_a, ex_a, ez_a, es_a by the names 'vx' .. 'es'):
+        ([nshot, nt] src_wav_a, dict field -> [nshot, nt, nz_t, nx_t]), frame n
+        = the carry out of adjoint step n, in forward-time order."""
+        mask = self._field_mask(fields)
+        order = [f for f in N.FRAME_BITS if mask & N.FRAME_BITS[f]]
+        arr, keep = (out, out) if out is not None else self._frames_buffer(len(order))
+        ptr = arr.ctypes.data if isinstance(arr, np.ndarray) else arr.data_ptr()
+        sa = np.zeros((max(self.nshot, 1), self.nt), dtype=np.float32)
+        self._ok(self.lib.stfwi_adjoint_frames(self.h, mask, ptr, sa.ctypes.data, _stream()), "adjoint_frames")
+        self.check()
+        return sa, {f: arr[:, order.index(f)] for f in fields}, keep
+
     KERNELS = ("fwd_vel", "fwd_str", "adj_a", "adj_b")
 
     def profile(self, every):
@@ -285,6 +335,39 @@ class Solver:
                  "illumination")
         self.check()
         return ws
+
+
+def imaging_condition_device(Vs, Vp, rho, ex_hist, ez_hist, es_hist, U_a_hist, V_a_hist, dx, dz, dt, pad,
+                             free_surface, nz_dom, nx_dom, vx_hist=None, vz_hist=None, time_chunk=64):
+    """fwi/imaging.py:83-169 through stfwi_imaging_condition: histories
+    [nt, nz_t, nx_t] (NumPy or torch, host or CUDA; cast to float32), FP64
+    time sums on the GPU.  Returns six [nz_dom, nx_dom] FP64 arrays (g_Vs,
+    g_Vp, g_rho, g_lam, g_mu, g_rho_lame)."""
+    lib = N.load()
+    if (vx_hist is None) != (vz_hist is None):
+        raise ValueError("give both vx_hist and vz_hist, or neither")
+    nt = int(U_a_hist.shape[0])
+    nz_t = nz_dom + pad if free_surface else nz_dom + 2 * pad
+    for name, h in (("ex_hist", ex_hist), ("ez_hist", ez_hist), ("es_hist", es_hist), ("U_a_hist", U_a_hist),
+                    ("V_a_hist", V_a_hist), ("vx_hist", vx_hist), ("vz_hist", vz_hist)):
+        if h is not None and tuple(h.shape) != (nt, nz_t, nx_dom + 2 * pad):
+            raise ValueError(f"{name} has shape {tuple(h.shape)}, expected {(nt, nz_t, nx_dom + 2 * pad)}")
+    bufs = [_as_buffer(a, np.float32) for a in (Vs, Vp, rho, ex_hist, ez_hist, es_hist, U_a_hist, V_a_hist)]
+    vel = [(None, None) if a is None else _as_buffer(a, np.float32) for a in (vx_hist, vz_hist)]
+    d = N.StfwiImagingDesc(int(nz_dom), int(nx_dom), int(pad), int(bool(free_surface)), nt, int(time_chunk),
+                           float(dx), float(dz), float(dt))
+    g = np.zeros((6, nz_dom, nx_dom), dtype=np.float64)
+    st = lib.stfwi_imaging_condition(ct.byref(d), *[b[0] for b in bufs], vel[0][0], vel[1][0], g.ctypes.data,
+                                     _stream())
+    if st == N.STFWI_ERR_INVALID:
+        raise ValueError("stfwi_imaging_condition: invalid arguments (see stderr)")
+    if st != N.STFWI_OK:
+        raise N.StfwiError(st, "stfwi_imaging_condition failed (see stderr)")
+    t = _torch()
+    if t is not None and t.cuda.is_available() and t.cuda.is_initialized():
+        t.cuda.current_stream().synchronize()
+    del bufs, vel
+    return tuple(g)
 
 
 def project_velocity_device(Vs, Vp, rho, K_margin=0.04, vp_cap=None, vs_floor=1e-3, rho_floor=1e-3):

@@ -75,8 +75,8 @@ def test_forward_and_adjoint_signatures_match_oracle():
     ref, _, _ = O.forward(vs, vp, rho, sx, 0, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, C.NT, C.FC, C.PAD, s_in, 8,
                           True, "force", d0_f32=True)
     assert _rel(vz, ref[1]) < 1e-5 and _rel(ex, ref[2]) < 1e-5
-    with pytest.raises(NotImplementedError):
-        fwi.build_forward_fn(C.NZ, C.NX, C.DX, C.DZ, C.DT, C.NT, C.FC, C.PAD, 100, rx, rz, return_vars=["vx_full"])
+    with pytest.raises(ValueError):
+        fwi.build_forward_fn(C.NZ, C.NX, C.DX, C.DZ, C.DT, C.NT, C.FC, C.PAD, 100, rx, rz, return_vars=["vy_full"])
     with pytest.raises(NotImplementedError):
         fwi.adjoint_jax(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, C.NT, C.FC, C.PAD, *ys,
                         fd_order=6)

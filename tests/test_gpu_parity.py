@@ -372,3 +372,45 @@ def test_autotuned_schedule_gives_the_same_gradient():
         S.close()
     for a, b in zip(res[1], res[0]):
         assert _rel(a, b) < 1e-6, _rel(a, b)
+
+
+def test_config1_single_shot_gradient_vs_oracle():
+    """The single-shot configuration at full size: 152 x 500 at 20 m, fd 4,
+    20-cell C-PML with a free surface, 2000 steps of 1.5 ms, one Ricker (5 Hz)
+    vertical force at 40 m depth and x = 5000 m, 250 receivers at 20 m depth
+    recording vx and vz.  Observed data: the FP64 oracle on the seeded
+    layered-fault model; start: that model smoothed (sigma 10 cells).  The
+    GPU's traces, FP64 misfit and exact g_Vs on the start model against the
+    FP64 oracle's."""
+    from stfwi_b200 import models as Mo
+    cfg = Mo.CONFIG1
+    nz, nx, nt, dt, fc, pad, fd = cfg["nz"], cfg["nx"], cfg["nt"], cfg["dt"], cfg["fc"], cfg["pad"], cfg["fd_order"]
+    true = Mo.layered_fault_model(nz, nx, seed=1)
+    init = Mo.smooth_initial(*true, sigma=10.0)
+    sx, sz, types, rx, rz = Mo.acquisition(cfg)
+    wav = Mo.ricker(np.arange(nt) * dt, fc, 1.5 / fc)
+    geo = dict(rec_x=rx, rec_z=rz, nx_dom=nx, nz_dom=nz, dx=cfg["dx"], dz=cfg["dz"], dt=dt, nt=nt, fc=fc,
+               pad=pad, fd_order=fd, free_surface=True, d0_f32=True)
+    obs = O.forward_batch(*true, sx, sz, types, src_wavelet=wav, **geo)[:, 1]
+    ref_rec = O.forward_batch(*init, sx, sz, types, src_wavelet=wav, **geo)
+    (g_ref, _, _), loss = O.compute_gradient("ad", Vs=init[0], Vp=init[1], rho=init[2], src_x=sx, src_z=sz,
+                                             src_wavelet=wav, observed=obs, src_types=types, component=1,
+                                             scale=1.0, invert="vs", **geo)
+    S = _solver(nt, len(rx), 1, fd, True, want_gradient=True, pad=pad, nz=nz, nx=nx, dx=cfg["dx"],
+                dz=cfg["dz"], dt=dt, fc=fc)
+    S.set_model(*init)
+    S.set_receivers(rx, rz)
+    S.set_shots(sx, sz, types, wav.astype(np.float32))
+    S.forward(store=True)
+    rec = S.records()
+    mis = S.misfit(obs.astype(np.float32), 1, 1.0)
+    g = S.gradient(exact=True)["exact"][0]
+    S.close()
+    e_rec = max(_rel(rec[0, c], ref_rec[0, c]) for c in range(2))
+    amp = float(np.linalg.norm(rec[0, 1]) / np.linalg.norm(rec[0, 1] - obs[0]))
+    e_mis, e_g = abs(mis.sum() / loss - 1), _rel(g, g_ref)
+    print(f"config 1 (fd4, 2000 steps): vx/vz traces rel-L2 {e_rec:.2e}, amplification {amp:.1f}, "
+          f"misfit rel {e_mis:.2e}, g_Vs rel-L2 {e_g:.2e}")
+    assert e_rec < 1e-5, e_rec
+    tol = 2e-5 * max(amp, 1.0)
+    assert e_mis < tol and e_g < tol, (e_mis, e_g, tol)

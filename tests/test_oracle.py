@@ -176,3 +176,25 @@ def test_known_answers_gradient_compare(known_answers):
     assert abs(loss_hc / K["gc_loss_HC"] - 1) < 1e-10
     ref = K["gc_g_Vs_HC"].astype(np.float64)
     assert np.linalg.norm(g_hc - ref) / np.linalg.norm(ref) < 1e-7
+
+
+@pytest.mark.parametrize("fs", [True, False])
+def test_history_imaging_formula_matches_fused_sums(fs):
+    """oracle.imaging_condition (fwi/imaging.py:83-169 on full histories, with
+    np.roll) against the imaging sums fused into the oracle's adjoint sweep:
+    the two restatements of the same formula agree to FP64 rounding."""
+    vs, vp, rho = C.model()
+    nt, st, fd = 30, "moment", 8
+    sx, sz, rx, rz = C.acquisition(fs, st)
+    wav = O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9
+    rng = np.random.default_rng(5)
+    ys = [rng.standard_normal((nt, len(rx))) for _ in range(4)]
+    _, full, _ = O.forward(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, nt, C.FC, C.PAD, wav, fd, fs,
+                           st, full=("vx", "vz", "ex", "ez", "es"))
+    a = O.adjoint(vs, vp, rho, sx, sz, rx, rz, C.NX, C.NZ, C.DX, C.DZ, C.DT, nt, C.FC, C.PAD, *ys, fd_order=fd,
+                  free_surface=fs, src_type=st, src_wavelet=wav, want=("img",), hist=("U_a", "V_a"))
+    g = O.imaging_condition(vs, vp, rho, full["ex"], full["ez"], full["es"], a["U_a"], a["V_a"], C.DX, C.DZ, C.DT,
+                            C.PAD, fs, C.NZ, C.NX, vx_hist=full["vx"], vz_hist=full["vz"])
+    for k, p in enumerate(a["img"]):
+        ref = O.crop(p, C.PAD, fs, C.NZ, C.NX)
+        np.testing.assert_allclose(g[3 + k], ref, rtol=0, atol=1e-11 * np.abs(ref).max())
