@@ -150,6 +150,13 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
  * padded grid, [nz_t][nx_t] FP64 (runs its own forward). */
 stfwi_status stfwi_illumination(stfwi_handle *h, int32_t component, double *ws_out, void *stream);
 
+/* Polls of a tile-copy wait before the kernel gives up, records
+ * STFWI_ERR_TIMEOUT for stfwi_check and returns (no counterpart in the
+ * reference).  polls < 0 restores the default (2^22); 0 makes every wait
+ * give up at once, which is how the tests exercise the timeout path without
+ * a GPU fault.  Values above the default are clamped to it. */
+stfwi_status stfwi_set_wait_limit(stfwi_handle *h, int64_t polls);
+
 /* Synchronises the stream and returns the device status word (0 = fine). */
 stfwi_status stfwi_check(stfwi_handle *h, void *stream);
 

@@ -27,7 +27,7 @@ EXPORTS = (
     "stfwi_set_adjoint_sources", "stfwi_gradient", "stfwi_illumination", "stfwi_check",
     "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
     "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
-    "stfwi_forward_frames", "stfwi_adjoint_frames", "stfwi_imaging_condition",
+    "stfwi_forward_frames", "stfwi_adjoint_frames", "stfwi_imaging_condition", "stfwi_set_wait_limit",
 )
 
 # full wavefield frames (bit set, in this order)
@@ -118,6 +118,7 @@ def load():
         L.stfwi_project_velocity.argtypes = [ct.c_int64, vp, vp, vp, f64, f64, f64, f64, vp]
         L.stfwi_autotune.argtypes = [H, i32, vp, vp]
         L.stfwi_forward_frames.argtypes = [H, u32, vp, vp]
+        L.stfwi_set_wait_limit.argtypes = [H, ct.c_int64]
         L.stfwi_adjoint_frames.argtypes = [H, u32, vp, vp, vp]
         L.stfwi_imaging_condition.argtypes = [ct.POINTER(StfwiImagingDesc)] + [vp] * 10 + [vp, vp]
         sz, f32 = ct.c_size_t, ct.c_float

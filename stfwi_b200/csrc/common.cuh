@@ -52,6 +52,7 @@ struct Geo {
     long long zstride;         // zs_n*P   (one z-psi array)
     long long nd;              // nz_dom*nx_dom
     int snf;                   // history fields per slot: 3 (stresses) or 5 (+ U, V)
+    uint32_t wait_polls;       // mbarrier polls before a tile wait gives up (WAIT3 by default)
 };
 
 struct Mat {
@@ -172,16 +173,15 @@ struct Ctx3 {
     int tile, j0, i0, s0, s1;
 };
 
-// on a wait that ran out: record the timeout and drain this block's copies
-// still in flight (bounded too) before the block returns
-__device__ __forceinline__ void abort3(uint64_t *bar, int nbar, int *status)
+// on a wait that ran out (the copy of shot `it` of the block): record the
+// timeout and, before the block returns, drain the copies still in flight,
+// which are those of shots it and it + 1 (each shot's copy is issued two
+// shots ahead, on barrier it & 1); these waits are bounded too
+__device__ __forceinline__ void abort3(uint64_t *bar, int it, int nsh, int *status)
 {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicOr(status, ST_TIMEOUT3);
-        for (int b = 0; b < nbar; ++b) {
-            mbar_wait_bounded(bar + b, 0, WAIT3);
-            mbar_wait_bounded(bar + b, 1, WAIT3);
-        }
+        for (int k = it; k < it + 2 && k < nsh; ++k) mbar_wait_bounded(bar + (k & 1), (k >> 1) & 1, WAIT3);
     }
 }
 

@@ -325,8 +325,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         const float *own = S + T::S3;   // [U, V][TZH][TX4] of the tile's own cells
         float *U = F + ((long long)s * F_N + F_U) * g.fstride;
         float *V = F + ((long long)s * F_N + F_V) * g.fstride;
-        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
-            abort3(bar, 2, status);
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, g.wait_polls))) {
+            abort3(bar, it, nsh, status);
             return;
         }
         const float *sxx = S, *szz = S + SN, *sxz = S + 2 * SN;
@@ -496,8 +496,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         float *sxx = F + ((long long)s * F_N + F_EX) * g.fstride;
         float *szz = F + ((long long)s * F_N + F_EZ) * g.fstride;
         float *sxz = F + ((long long)s * F_N + F_ES) * g.fstride;
-        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
-            abort3(bar, 2, out.status);
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, g.wait_polls))) {
+            abort3(bar, it, nsh, out.status);
             return;
         }
         const float *sU = S, *sV = S + SN;
@@ -725,8 +725,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         const float *own = S + T::S3;   // [P, Q][TZH][TX4] of the tile's own cells
         float *Pp = A + ((long long)s * F_N + F_U) * g.fstride;
         float *Qp = A + ((long long)s * F_N + F_V) * g.fstride;
-        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
-            abort3(bar, 2, status);
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, g.wait_polls))) {
+            abort3(bar, it, nsh, status);
             return;
         }
         if (fix) {
@@ -990,8 +990,8 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                                     ? o.snap + ((long long)s * o.slots + o.slot_img) * g.snf * g.nd : nullptr;
         const float *snap_next = (IMG && RHO && o.slot_next >= 0)
                                      ? o.snap + ((long long)s * o.slots + o.slot_next) * g.snf * g.nd : nullptr;
-        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, WAIT3))) {
-            abort3(bar, 2, status);
+        if (!__syncthreads_and(mbar_wait_bounded(bar + (it & 1), (it >> 1) & 1, g.wait_polls))) {
+            abort3(bar, it, nsh, status);
             return;
         }
         if (fix) {

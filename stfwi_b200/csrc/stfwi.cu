@@ -977,6 +977,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.dtdxdz = (float)(d->dt / (d->dx * d->dz));
     g.fstride = p.nz * p.P; g.xstride = p.nz * p.xs_n; g.zstride = p.zs_n * p.P; g.nd = p.nd;
     g.snf = d->want_gradient == 2 ? 5 : 3;
+    g.wait_polls = WAIT3;
     h->accp = g.snf == 5 ? 7 : 5;
     h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
     h->ntx = (int)((p.nx + h->tw - 1) / h->tw);
@@ -1632,6 +1633,17 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
     h->stored = false;   // the timing passes overwrote the state
     if (spg_out)
         for (int k = 0; k < 4; ++k) spg_out[k] = pick[k];
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_wait_limit(stfwi_handle *h, int64_t polls)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    const uint32_t v = polls < 0 ? WAIT3 : (uint32_t)std::min<int64_t>(polls, WAIT3);
+    if (v != h->g.wait_polls) {
+        h->g.wait_polls = v;
+        drop_graphs(h);   // the limit is a kernel argument baked into the captured graphs
+    }
     return STFWI_OK;
 }
 

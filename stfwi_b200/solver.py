@@ -277,6 +277,11 @@ class Solver:
         self.check()
         return sa, {f: arr[:, order.index(f)] for f in fields}, keep
 
+    def set_wait_limit(self, polls=-1):
+        """Polls of a tile-copy wait before a kernel gives up with
+        STFWI_ERR_TIMEOUT (-1: the default; 0: every wait gives up at once)."""
+        self._ok(self.lib.stfwi_set_wait_limit(self.h, int(polls)), "set_wait_limit")
+
     KERNELS = ("fwd_vel", "fwd_str", "adj_a", "adj_b")
 
     def profile(self, every):
