@@ -44,9 +44,12 @@ def features(g_raw, precond, vp, vs):
                      (np.asarray(vs, np.float64) - 1700.0) / 500.0]).astype(np.float32)
 
 
-def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
+def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print, method="reference"):
     """Training pairs of the given model seeds: (inputs [n, 4, nz, nx],
-    targets [n, nz, nx] in units of TARGET_SCALE, seconds spent)."""
+    targets [n, nz, nx] in units of TARGET_SCALE, seconds spent).  The
+    update is what ``n_iter`` iterations of the plain method make:
+    ``method='reference'`` the reference's L-BFGS (``I.lbfgs_reference``),
+    ``'armijo'`` the backtracking variant (``I.lbfgs``)."""
     X, Y = [], []
     t0 = time.perf_counter()
     batch = I.ModelBatch(K, geom)
@@ -64,7 +67,10 @@ def generate_pairs(seeds, K=4, n_iter=10, geom=I.GEOMETRY, log=print):
 
                 def rec(x, f, graw, k=k):
                     first.setdefault(k, graw.copy())
-                gens.append(I.lbfgs(models[k][1][0], batch.vp[k], batch.precond[k], n_iter, record=rec))
+                if method == "reference":
+                    gens.append(I.lbfgs_reference(models[k][1][0], batch.precond[k], n_iter, record=rec))
+                else:
+                    gens.append(I.lbfgs(models[k][1][0], batch.vp[k], batch.precond[k], n_iter, record=rec))
             finals, _ = I.run_lockstep(batch, gens)
             for k in range(len(group)):
                 init = models[k][1]
@@ -233,6 +239,124 @@ def evaluate(net, seeds, K=4, n_plain=20, geom=I.GEOMETRY, alphas=(1.0, 0.5, 0.2
     return out
 
 
+BANDS = (3.0, 5.0, 8.0)   # the multiscale schedule's low-pass cutoffs (Hz), 20 iterations each
+
+
+def evaluate_multiband(net, seeds, K=4, bands=BANDS, iters=20, geom=I.GEOMETRY, alphas=(1.0, 0.5, 0.25),
+                       log=print):
+    """Learned vs plain on held-out models over the multiscale schedule.
+
+    Plain (the fallback and the judge): for each band in turn, the misfit
+    filter is set to its cutoff, the illumination preconditioner is
+    recomputed at the current Vs, and the reference's L-BFGS
+    (``I.lbfgs_reference``: history 100, 5 % step cap, strong Wolfe line
+    search of at most 40 evaluations) runs ``iters`` iterations.  Its lowest
+    Vs relative-RMS error over the whole schedule is the model's target.
+    Learned: the same schedule, except that the first band starts with the
+    network's direction (accepted only if a misfit line search over
+    ``alphas`` lowers the misfit, otherwise the plain method starts from the
+    initial model); it stops as soon as the Vs error reaches the target.
+    Both clocks count the GPU rounds, the preconditioners and the network.
+    Vp and rho are the true ones, as in the reference's Vs-only driver
+    (Main_ex_Vs.py:203-205 keeps the true Vp and rho when no stage inverts
+    them)."""
+    import torch
+    out = []
+    batch = I.ModelBatch(K, dict(geom, cutoff=bands[0]))
+    try:
+        for g0 in range(0, len(seeds), K):
+            group = list(seeds[g0:g0 + K])
+            models = [I.true_and_initial(s, geom) for s in group]
+            slots = list(range(len(group)))
+            for k in slots:
+                batch.load(k, *models[k])
+            true_vs = {k: models[k][0][0] for k in slots}
+            vs0 = {k: models[k][1][0].astype(np.float64) for k in slots}
+
+            def band_runs(start, hist, clock, stop_at=None, first_band_start=None):
+                """Run the bands from Vs `start`; returns the final Vs per slot."""
+                cur = dict(start)
+                for b, cut in enumerate(bands):
+                    live = [k for k in slots if not (stop_at and hist[k] and hist[k][-1][1] <= stop_at[k])]
+                    if not live:
+                        break
+                    batch.set_cutoff(cut)
+                    t0 = time.perf_counter()
+                    batch.refresh_precond([cur[k] if k in live else None for k in range(K)])
+                    clock["t"] += time.perf_counter() - t0
+                    if b == 0 and first_band_start is not None:
+                        cur.update(first_band_start(live, clock))
+                    gens = []
+                    for k in range(K):
+                        if k not in live:
+                            gens.append(None)
+                            continue
+                        st = (lambda x, f, k=k: I.vs_rel_rms(x, true_vs[k]) <= stop_at[k]) if stop_at else None
+                        gens.append(I.lbfgs_reference(cur[k], batch.precond[k], iters, stop=st,
+                                                      record=lambda x, f, g, k=k: hist[k].append(
+                                                          (clock["t"], I.vs_rel_rms(x, true_vs[k]), f))))
+                    finals, _ = I.run_lockstep(batch, gens, clock)
+                    for k in live:
+                        cur[k] = finals[k]
+                return cur
+
+            clock = {"t": 0.0}
+            plain = {k: [] for k in slots}
+            band_runs(vs0, plain, clock)
+            target = {k: min(e for _, e, _ in plain[k]) for k in slots}
+
+            learned = {k: [] for k in slots}
+            accepted, step = {}, {}
+            t_net = [0.0]
+
+            def learned_start(live, clock):
+                t0 = time.perf_counter()
+                res = batch.evaluate([vs0[k] if k in live else None for k in range(K)])
+                clock["t"] += time.perf_counter() - t0
+                f0 = {k: res[k][0] for k in live}
+                t0 = time.perf_counter()
+                X = np.stack([features(res[k][1], batch.precond[k], batch.vp[k], vs0[k]) for k in live])
+                d = predict(net, X) * TARGET_SCALE
+                torch.cuda.synchronize()
+                t_net[0] = time.perf_counter() - t0
+                clock["t"] += t_net[0]
+                dk = {k: d[i] for i, k in enumerate(live)}
+                for a in alphas:
+                    cand = [I.project_vs(vs0[k] + a * dk[k], batch.vp[k]) if (k in live and k not in accepted)
+                            else None for k in range(K)]
+                    if all(c is None for c in cand):
+                        break
+                    t0 = time.perf_counter()
+                    fs = batch.misfits(cand)
+                    clock["t"] += time.perf_counter() - t0
+                    for k in live:
+                        if cand[k] is not None and fs[k] < f0[k]:
+                            accepted[k], step[k] = cand[k], a
+                            learned[k].append((clock["t"], I.vs_rel_rms(cand[k], true_vs[k]), fs[k]))
+                return {k: accepted[k] for k in live if k in accepted}
+
+            clock = {"t": 0.0}
+            for k in slots:
+                learned[k].append((0.0, I.vs_rel_rms(vs0[k], true_vs[k]), float("nan")))
+            band_runs(vs0, learned, clock, stop_at=target, first_band_start=learned_start)
+            for k in slots:
+                tp = _first_time(plain[k], target[k])
+                tl = _first_time(learned[k], target[k])
+                rec = dict(seed=int(group[k]), err_start=plain[k][0][1], target=target[k],
+                           plain_time_s=tp, learned_time_s=tl,
+                           ratio=(tl / tp) if (tl is not None and tp) else None,
+                           learned_step_accepted=k in accepted, step=step.get(k),
+                           err_after_learned_step=I.vs_rel_rms(accepted[k], true_vs[k]) if k in accepted else None,
+                           err_plain_final=plain[k][-1][1], err_learned_final=learned[k][-1][1],
+                           plain_iterates=len(plain[k]), learned_iterates=len(learned[k]),
+                           network_s=t_net[0] / len(group), bands=list(bands), iters_per_band=iters)
+                out.append(rec)
+                log(json.dumps(rec))
+    finally:
+        batch.close()
+    return out
+
+
 def summarize(records):
     ratios = [r["ratio"] for r in records if r["ratio"] is not None]
     after = [r["err_after_learned_step"] for r in records if r["err_after_learned_step"] is not None]
@@ -255,6 +379,10 @@ def main(argv=None):
     ap.add_argument("--val", type=int, default=16, help="training pairs held out for validation")
     ap.add_argument("--K", type=int, default=4, help="models evaluated concurrently")
     ap.add_argument("--out", default="learned_out")
+    ap.add_argument("--method", default="reference", choices=["reference", "armijo"],
+                    help="plain optimizer of the training pairs")
+    ap.add_argument("--multiband", action="store_true",
+                    help="evaluate over the 3/5/8 Hz schedule (reference L-BFGS as the plain arm)")
     ap.add_argument("--weights", default=None,
                     help="evaluate these trained weights (save_weights format) instead of generating data and training")
     a = ap.parse_args(argv)
@@ -276,14 +404,18 @@ def _run(a, logf):
         t_data = t_train = 0.0
         hist, best_epoch, zero_val = [], None, None
     else:
-        X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log)
+        X, Y, t_data = generate_pairs(list(range(1000, 1000 + a.train)), K=a.K, n_iter=a.iters, log=log,
+                                      method=a.method)
         n_val = min(a.val, X.shape[0] // 4)
         t0 = time.perf_counter()
         net, hist, best_epoch = train(X, Y, epochs=a.epochs, n_val=n_val, log=log)
         t_train = time.perf_counter() - t0
         zero_val = float(np.mean(Y[X.shape[0] - n_val:].astype(np.float64) ** 2)) if n_val else None
         save_weights(os.path.join(a.out, "unet_weights.npz"), net.params.detach().cpu().numpy())
-    recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
+    if a.multiband:
+        recs = evaluate_multiband(net, list(range(5000, 5000 + a.test)), K=a.K, iters=a.plain, log=log)
+    else:
+        recs = evaluate(net, list(range(5000, 5000 + a.test)), K=a.K, n_plain=a.plain, log=log)
     summary = dict(config=dict(vars(a), geometry=I.GEOMETRY), data_seconds=t_data, train_seconds=t_train,
                    train_history=hist, best_epoch=best_epoch, val_loss_of_zero_prediction=zero_val,
                    evaluation=summarize(recs), records=recs)

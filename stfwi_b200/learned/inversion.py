@@ -131,6 +131,163 @@ def lbfgs(vs0, vp, precond, n_iter, mem=10, step0=50.0, c1=1e-4, max_ls=6, recor
     return x
 
 
+def _cubic_min(a, fa, da, b, fb, db):
+    """Minimiser of the cubic through (a, fa, fa') and (b, fb, fb'), or None
+    (Nocedal and Wright, eq. 3.59)."""
+    d1 = da + db - 3.0 * (fa - fb) / (a - b)
+    disc = d1 * d1 - da * db
+    if disc < 0.0:
+        return None
+    d2 = np.copysign(np.sqrt(disc), b - a)
+    den = db - da + 2.0 * d2
+    if den == 0.0:
+        return None
+    return b - (b - a) * (db + d2 - d1) / den
+
+
+def strong_wolfe_search(f0, slope0, init_step, max_step, maxls=40, c1=1e-4, c2=0.9):
+    """Line search for the strong Wolfe conditions (Nocedal and Wright,
+    Algorithms 3.5 and 3.6: bracketing, then zoom with safeguarded cubic
+    interpolation), as a generator: yields a step length, receives
+    (f, slope) there; at most ``maxls`` evaluations.  Returns (step, ok):
+    the first step meeting both conditions, else the best step meeting
+    sufficient decrease (0.0 when none did)."""
+    a_prev, f_prev, s_prev = 0.0, f0, slope0
+    a = min(init_step, max_step)
+    best = (0.0, f0)
+    n = 0
+
+    def decrease(a_, f_):
+        return f_ <= f0 + c1 * a_ * slope0
+
+    def zoom(lo, flo, slo, hi, fhi, shi):
+        nonlocal n, best
+        while n < maxls:
+            t = _cubic_min(lo, flo, slo, hi, fhi, shi)
+            lo_b, hi_b = min(lo, hi), max(lo, hi)
+            w = hi_b - lo_b
+            if t is None or not (lo_b + 0.1 * w <= t <= hi_b - 0.1 * w):
+                t = 0.5 * (lo + hi)
+            ft, st = yield t
+            n += 1
+            if decrease(t, ft) and ft < best[1]:
+                best = (t, ft)
+            if not decrease(t, ft) or ft >= flo:
+                hi, fhi, shi = t, ft, st
+            else:
+                if abs(st) <= -c2 * slope0:
+                    return t, True
+                if st * (hi - lo) >= 0.0:
+                    hi, fhi, shi = lo, flo, slo
+                lo, flo, slo = t, ft, st
+        return best[0], False
+
+    while n < maxls:
+        fa, sa = yield a
+        n += 1
+        if decrease(a, fa) and fa < best[1]:
+            best = (a, fa)
+        if not decrease(a, fa) or (n > 1 and fa >= f_prev):
+            return (yield from zoom(a_prev, f_prev, s_prev, a, fa, sa))
+        if abs(sa) <= -c2 * slope0:
+            return a, True
+        if sa >= 0.0:
+            return (yield from zoom(a, fa, sa, a_prev, f_prev, s_prev))
+        if a >= max_step:
+            return a, False          # the largest step still descends: take it
+        a_prev, f_prev, s_prev = a, fa, sa
+        a = min(2.0 * a, max_step)
+    return best[0], False
+
+
+def lbfgs_reference(vs0, precond, n_iter, history_size=100, step_pct=0.05, maxls=40, smooth_sigma=1.0,
+                    increase=1.5, record=None, stop=None):
+    """The reference's plain inversion loop on Vs (fwi/optimizer.py:20-168
+    run_lbfgs with a Vs-only loss from fwi/loss.py build_loss_fn, as
+    Main_ex_Vs.py drives it), restated as a generator: yields the next Vs
+    to evaluate and receives (misfit, raw g_Vs).
+
+    * the gradient L-BFGS sees is the raw one Gaussian-smoothed (sigma
+      ``smooth_sigma``) and multiplied by the illumination preconditioner
+      (fwi/loss.py, ``_postprocess`` of fwi/gradient.py:266-277);
+    * every iteration caps the step length at step_pct * max|Vs| / max|g|
+      (fwi/optimizer.py:96-106, recomputed each epoch at :124-131);
+    * the direction comes from the two-loop recursion over the last
+      ``history_size`` pairs with the initial matrix s'y / y'y (the jaxopt
+      LBFGS the reference uses, history 100); the first is -g;
+    * the step is found by a strong Wolfe line search of at most ``maxls``
+      evaluations (maxls=40, :110-111), starting from ``increase`` times
+      the previous step (jaxopt's "increase" initialisation), the first from
+      the cap; if it fails, the best sufficient-decrease step is taken (none:
+      the iterate stays).
+    No bounds, as in the reference.  ``record(vs, f, g_raw)`` sees every
+    accepted iterate (and the start); ``stop(vs, f)`` ends early."""
+    from ..fwi.loss import gaussian_smooth_2d
+    P = np.asarray(precond, np.float64)
+
+    def direction(graw):
+        g = graw if not smooth_sigma else gaussian_smooth_2d(graw, smooth_sigma)
+        return np.asarray(g, np.float64) * P
+
+    x = np.asarray(vs0, np.float64).copy()
+    f, graw = yield x
+    g = direction(graw)
+    if record:
+        record(x, f, graw)
+    if stop and stop(x, f):
+        return x
+    S, Y, RHO = [], [], []
+    gamma = 1.0
+    step = None
+    for _ in range(n_iter):
+        max_step = step_pct * float(np.abs(x).max()) / (float(np.abs(g).max()) + 1e-30)
+        q = g.copy()
+        alphas = []
+        for s, y, r in zip(reversed(S), reversed(Y), reversed(RHO)):
+            a = r * float(np.vdot(s, q))
+            q -= a * y
+            alphas.append(a)
+        q *= gamma
+        for (s, y, r), a in zip(zip(S, Y, RHO), reversed(alphas)):
+            b = r * float(np.vdot(y, q))
+            q += s * (a - b)
+        d = -q
+        slope0 = float(np.vdot(g, d))
+        if slope0 >= 0.0:          # not a descent direction: steepest descent
+            d = -g
+            slope0 = float(np.vdot(g, d))
+        init = max_step if step is None else increase * step
+        ls = strong_wolfe_search(f, slope0, init, max_step, maxls=maxls)
+        trial = {}
+        try:
+            a = next(ls)
+            while True:
+                xa = x + a * d
+                fa, graw_a = yield xa
+                ga = direction(graw_a)
+                trial[a] = (xa, fa, graw_a, ga)
+                a = ls.send((fa, float(np.vdot(ga, d))))
+        except StopIteration as e:
+            a_ok, _ok = e.value
+        if a_ok <= 0.0 or a_ok not in trial:
+            step = step if step is not None else max_step
+            continue                   # no decrease found: the iterate stays
+        xn, fn, graw_n, gn = trial[a_ok]
+        s, y = xn - x, gn - g
+        sy = float(np.vdot(s, y))
+        if sy > 0.0:
+            S.append(s); Y.append(y); RHO.append(1.0 / sy)
+            if len(S) > history_size:
+                S.pop(0); Y.pop(0); RHO.pop(0)
+            gamma = sy / float(np.vdot(y, y))
+        x, f, g, step = xn, fn, gn, a_ok
+        if record:
+            record(x, f, graw_n)
+        if stop and stop(x, f):
+            return x
+    return x
+
+
 def run_lockstep(batch, gens, clock=None):
     """Drive one generator per slot (None for idle slots) until all finish;
     every round evaluates the Vs each live generator yielded.  ``clock['t']``
@@ -225,6 +382,28 @@ class ModelBatch:
             self.precond[k] = S.preconditioner("illum", comp, 1e-3)
         st.synchronize()
 
+    def set_cutoff(self, cutoff):
+        """Low-pass cutoff (Hz) of the misfit filter for the following
+        evaluations (an order-6 Butterworth; None: unfiltered)."""
+        from scipy.signal import butter
+        self.geom["cutoff"] = cutoff
+        self.sos = butter(6, cutoff, fs=1.0 / self.geom["dt"], output="sos") if cutoff else None
+
+    def refresh_precond(self, vs_list, eps=1e-3):
+        """Illumination preconditioner of each slot at its current Vs (the
+        reference recomputes it at the start of every stage,
+        Main_ex_Vs.py:237-247); None entries keep theirs."""
+        torch = self.torch
+        for k, vs in enumerate(vs_list):
+            if vs is None:
+                continue
+            S = self.solvers[k]
+            with torch.cuda.stream(self.streams[k]):
+                S.set_model(np.asarray(vs, np.float32), self.vp[k].astype(np.float32),
+                            self.rho[k].astype(np.float32))
+                self.precond[k] = S.preconditioner("illum", self.geom["component"], eps)
+        torch.cuda.synchronize()
+
     def _launch(self, k, vs, gradient):
         S = self.solvers[k]
         S.set_model(np.asarray(vs, np.float32), self.vp[k].astype(np.float32), self.rho[k].astype(np.float32))
@@ -246,8 +425,13 @@ class ModelBatch:
         torch.cuda.synchronize()
         out = [None] * len(vs_list)
         for k in active:
-            self.solvers[k].check()
-            out[k] = (float(self.mis[k].sum()), self.grad[k][0, 0].cpu().numpy())
+            try:
+                self.solvers[k].check()
+                out[k] = (float(self.mis[k].sum()), self.grad[k][0, 0].cpu().numpy())
+            except Exception as e:   # an unstable trial model: an infinite misfit for the line search
+                if getattr(e, "status", None) != 5:
+                    raise
+                out[k] = (float("inf"), np.zeros((self.geom["nz"], self.geom["nx"])))
         self.evals += len(active)
         return out
 
@@ -261,8 +445,13 @@ class ModelBatch:
         torch.cuda.synchronize()
         out = [None] * len(vs_list)
         for k in active:
-            self.solvers[k].check()
-            out[k] = float(self.mis[k].sum())
+            try:
+                self.solvers[k].check()
+                out[k] = float(self.mis[k].sum())
+            except Exception as e:
+                if getattr(e, "status", None) != 5:
+                    raise
+                out[k] = float("inf")
         return out
 
     def close(self):

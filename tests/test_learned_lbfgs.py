@@ -128,3 +128,65 @@ def test_acquisition_and_model_pair():
     (vs, vp, rho), (vs0, vp0, rho0) = I.true_and_initial(5000)
     assert vs.shape == (152, 500) and np.all(vs <= vp / 1.2 + 1e-3)
     assert I.vs_rel_rms(vs, vs) == 0.0 and 0.0 < I.vs_rel_rms(vs0, vs) < 0.2
+
+
+def _drive(gen, fg):
+    x = next(gen)
+    n = 1
+    try:
+        while True:
+            x = gen.send(fg(x))
+            n += 1
+    except StopIteration as e:
+        return e.value, n
+
+
+def test_reference_lbfgs_converges_and_caps_the_step():
+    """The restated reference optimizer (fwi/optimizer.py run_lbfgs: history
+    100, step cap step_pct * max|x| / max|g|, strong Wolfe line search of at
+    most 40 evaluations) on an ill-conditioned quadratic: it converges, every
+    accepted step meets sufficient decrease, and the first step moves no cell
+    by more than the cap."""
+    from stfwi_b200.learned import inversion as I
+    rng = np.random.default_rng(0)
+    shape = (8, 10)
+    diag = np.exp(rng.uniform(0, 4, shape))
+    b = rng.standard_normal(shape) * 5
+    x_star = b / diag
+
+    def fg(x):
+        return 0.5 * np.sum(diag * x * x) - np.sum(b * x), diag * x - b
+
+    x0 = np.full(shape, 1.5)
+    hist = []
+    gen = I.lbfgs_reference(x0, np.ones(shape), 60, smooth_sigma=0, step_pct=100.0,
+                            record=lambda x, f, g: hist.append((x.copy(), f)))
+    x, n = _drive(gen, fg)
+    assert np.abs(x - x_star).max() < 1e-5
+    assert all(hist[i + 1][1] < hist[i][1] for i in range(len(hist) - 1) if hist[i][1] - fg(x_star)[0] > 1e-9)
+    assert n < 2 * 60
+    # a 5 % cap: the first accepted step changes no cell by more than 5 % of max|x0|
+    hist = []
+    gen = I.lbfgs_reference(x0, np.ones(shape), 1, smooth_sigma=0, step_pct=0.05,
+                            record=lambda x, f, g: hist.append(x.copy()))
+    _drive(gen, fg)
+    assert len(hist) == 2
+    assert np.abs(hist[1] - hist[0]).max() <= 0.05 * 1.5 * (1 + 1e-12)
+
+
+def test_strong_wolfe_search_on_a_parabola():
+    """phi(a) = (a - 2)^2 from a = 0.5, capped at 10: the search returns a
+    step meeting both strong Wolfe conditions."""
+    from stfwi_b200.learned import inversion as I
+    phi = lambda a: ((a - 2.0) ** 2, 2.0 * (a - 2.0))
+    f0, s0 = phi(0.0)
+    ls = I.strong_wolfe_search(f0, s0, 0.5, 10.0)
+    a = next(ls)
+    try:
+        while True:
+            a = ls.send(phi(a))
+    except StopIteration as e:
+        step, ok = e.value
+    assert ok
+    f, s = phi(step)
+    assert f <= f0 + 1e-4 * step * s0 and abs(s) <= 0.9 * abs(s0)
