@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-every", type=int, default=20)
     p.add_argument("--no-autotune", action="store_true", help="keep the default shots per block")
+    p.add_argument("--variant", type=int, default=0, help="kernel family (stfwi_desc.kernel_variant)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-vs-plain time-to-Vs-error measurement (N = 1 only)")
     return p.parse_args()
@@ -264,7 +265,7 @@ def main():
     wav = Mo.ricker(np.arange(nt) * cfg["dt"], cfg["fc"], 1.5 / cfg["fc"]).astype(np.float32)
     S = Solver(cfg["nz"], cfg["nx"], cfg["dx"], cfg["dz"], cfg["dt"], nt, cfg["fc"], cfg["pad"],
                len(rx), ns, fd_order=cfg["fd_order"], free_surface=cfg["free_surface"],
-               want_gradient=True)
+               want_gradient=True, kernel_variant=args.variant)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav)
     comp = 1

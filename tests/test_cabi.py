@@ -84,7 +84,7 @@ def test_create_rejects_bad_descriptors_before_touching_a_device():
     d.pad, d.dt = 8, -1.0
     assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID
     d.dt = 1e-3
-    d.want_gradient, d.kernel_variant = 2, 1   # kernel_variant other than 0 is refused
+    d.want_gradient, d.kernel_variant = 2, 5   # an unknown kernel_variant is refused
     assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_UNSUPPORTED
     d.want_gradient, d.kernel_variant = 3, 0
     assert lib.stfwi_create(ct.byref(d), ct.byref(h)) == N.STFWI_ERR_INVALID

@@ -28,7 +28,7 @@ def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx
                   want_gradient=want_gradient, **kw)
 
 
-VARIANTS = [0]  # kernel families of the library (stfwi_desc.kernel_variant)
+VARIANTS = [0, 1]  # kernel families: two-column tiles, table-driven paired tiles (stfwi_desc.kernel_variant)
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
