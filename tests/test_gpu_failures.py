@@ -49,13 +49,19 @@ def _small_solver(nt=60, nshot=3, want_gradient=False):
 def test_wait_timeout_is_reported_and_the_handle_recovers():
     from stfwi_b200 import _native as N
     S, _, ref = _small_solver()
+    S.set_adjoint_sources(np.ones((3, 4, S.nt, S.nrec), dtype=np.float32))
+    # the forward kernels give up at their first wait
     S.set_wait_limit(0)
     S.forward()
     with pytest.raises(N.StfwiError) as e:
         S.check()
     assert e.value.status == N.STFWI_ERR_TIMEOUT
-    # the adjoint kernels report it the same way
-    S.set_adjoint_sources(np.ones((3, 4, S.nt, S.nrec), dtype=np.float32))
+    # a forward with the default limit clears the status; then the adjoint
+    # kernels give up the same way
+    S.set_wait_limit(-1)
+    S.forward()
+    S.check()
+    S.set_wait_limit(0)
     with pytest.raises(N.StfwiError) as e:
         S.gradient(exact=False, src=True)
     assert e.value.status == N.STFWI_ERR_TIMEOUT

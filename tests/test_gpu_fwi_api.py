@@ -150,5 +150,11 @@ def test_reference_first_gradient_34_shots(known_answers):
          "loss_HC": abs(loss_hc / K["fg_loss_HC"] - 1), "g_Vs_AD": _rel(g_ad, K["fg_g_Vs_AD"]),
          "g_Vs_HC": _rel(g_hc, K["fg_g_Vs_HC"])}
     print("first gradient (34 shots x 2890 steps):", {k: f"{v:.2e}" for k, v in e.items()})
-    assert e["auto_scale"] < 1e-4 and e["loss_AD"] < 1e-3 and e["loss_HC"] < 1e-3
-    assert e["g_Vs_AD"] < 1e-2 and e["g_Vs_HC"] < 1e-2
+    # measured on a B200: auto_scale 2.8e-7, losses 7.5e-7 / 1.6e-7, g_Vs_HC
+    # 6.9e-7 (FP32 stencils against the reference's FP64 run); bounds about 3x
+    assert e["auto_scale"] < 1e-6 and e["loss_AD"] < 3e-6 and e["loss_HC"] < 1e-6
+    assert e["g_Vs_HC"] < 2e-6
+    # g_Vs_AD was scaled by an illumination multiplier that the reference did
+    # not store; ours is rebuilt from its recipe (1.3e-3 measured), so this
+    # comparison carries that reconstruction, not the kernels' error
+    assert e["g_Vs_AD"] < 3e-3
