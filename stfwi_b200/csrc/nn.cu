@@ -30,6 +30,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 
@@ -644,15 +645,24 @@ int check_launch(const char *what)
 constexpr int NN_MAX_DEVICES = 64;
 
 // one pipeline error flag per device (a kernel writes the flag of its own device)
+// the status word of the pipeline waits: a device variable of this module,
+// zero when the module loads on a device; its address is looked up once per
+// device (under a lock), so no network op allocates or synchronises for it
+__device__ int g_nn_err_flag;
+
 int *err_flag()
 {
+    static std::mutex mu;
     static int *flags[NN_MAX_DEVICES] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NN_MAX_DEVICES) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
     if (!flags[dev]) {
         int *f = nullptr;
-        if (cudaMalloc(&f, sizeof(int)) != cudaSuccess) return nullptr;
-        cudaMemset(f, 0, sizeof(int));
+        if (cudaGetSymbolAddress((void **)&f, g_nn_err_flag) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
         flags[dev] = f;
     }
     return flags[dev];
@@ -731,7 +741,7 @@ int conv_common(const void *x, int n, int h, int w, int cin, const void *wt, int
     rc = encode_bf16(&tw, wt, 3, dw, bwx);
     if (rc) return rc;
     int *err = err_flag();
-    if (!err) return nn_fail(STFWI_ERR_OOM, "conv: error flag allocation failed");
+    if (!err) return nn_fail(STFWI_ERR_CUDA, "conv: the error flag of this device could not be looked up");
     static bool attr[NN_MAX_DEVICES] = {};
     rc = smem_limit_once(k_conv_kmajor, conv_smem(64, 128), attr, "conv: shared-memory attribute");
     if (rc) return rc;
@@ -756,7 +766,7 @@ const char *stfwi_nn_last_error(void) { return g_err.c_str(); }
 int stfwi_nn_check(void *stream)
 {
     int *err = err_flag();
-    if (!err) return nn_fail(STFWI_ERR_OOM, "error flag allocation failed");
+    if (!err) return nn_fail(STFWI_ERR_CUDA, "the error flag of this device could not be looked up");
     int v = 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cudaMemcpyAsync(&v, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -817,7 +827,7 @@ int stfwi_nn_conv3x3_wgrad(const void *x, const void *dz, int n, int h, int w, i
     rc = encode_bf16(&tb, x, 4, db, bb);
     if (rc) return rc;
     int *err = err_flag();
-    if (!err) return nn_fail(STFWI_ERR_OOM, "wgrad: error flag allocation failed");
+    if (!err) return nn_fail(STFWI_ERR_CUDA, "wgrad: the error flag of this device could not be looked up");
     static bool attr[NN_MAX_DEVICES] = {};
     rc = smem_limit_once(k_conv_wgrad, wgrad_smem(128), attr, "wgrad: shared-memory attribute");
     if (rc) return rc;
