@@ -53,6 +53,11 @@ struct Geo {
     long long nd;              // nz_dom*nx_dom
     int snf;                   // history fields per slot: 3 (stresses) or 5 (+ U, V)
     uint32_t wait_polls;       // mbarrier polls before a tile wait gives up (WAIT3 by default)
+    // dispatch order of the tiles of the staged tilings (A: fwd_vel, fwd_str,
+    // adj_a; B: adj_b): the `heavy` tiles that touch an edge, a C-PML strip
+    // or the free surface first, or null for the plain order
+    const int *tordA, *tordB;
+    int theavyA, theavyB;
 };
 
 struct Mat {

@@ -199,6 +199,33 @@ __device__ __forceinline__ void zwin2p(float2 (&w)[W], const float *s, int ty, i
     for (int m = 0; m < W; ++m) w[m] = *reinterpret_cast<const float2 *>(s + (ty * RPT + m) * SW4 + XO4 + 2 * tx);
 }
 
+// tile and shot group of this block, boundary tiles first: the blocks of
+// every (boundary tile, shot group) pair are dispatched before the interior
+// ones, so that the long blocks do not form the tail of the launch
+__device__ __forceinline__ Ctx3 ctx5(const Geo &g, int spg, int tzh, int tiles_x, const int *order, int heavy)
+{
+    const int tiles = gridDim.x, groups = gridDim.y;
+    const int b = blockIdx.y * tiles + blockIdx.x;
+    int t = blockIdx.x, grp = blockIdx.y;
+    if (order && heavy > 0 && heavy < tiles) {
+        if (b < heavy * groups) {
+            t = order[b % heavy];
+            grp = b / heavy;
+        } else {
+            const int b2 = b - heavy * groups, light = tiles - heavy;
+            t = order[heavy + b2 % light];
+            grp = b2 / light;
+        }
+    }
+    Ctx3 c;
+    c.tile = t;
+    c.j0 = (t % tiles_x) * TX4;
+    c.i0 = (t / tiles_x) * tzh;
+    c.s0 = grp * spg;
+    c.s1 = min(c.s0 + spg, g.nshot);
+    return c;
+}
+
 // shared-memory plans of the table-driven kernels: the two-column layout
 // followed by the coefficient tables (float4 per column of the tile for
 // each x-stencil set, per row of the tile for each z-stencil set)
@@ -228,7 +255,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     float4 *zt = xt + 2 * TX4;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::VEL);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
     if (nsh <= 0) return;
     if (tid == 0) {
@@ -417,7 +444,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     float4 *zt = xt + 2 * TX4;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::STR);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
     if (nsh <= 0) return;
     if (tid == 0) {
@@ -733,7 +760,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     float4 *zt = xt + 4 * TX4;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::ADA);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
     if (nsh <= 0) return;
     if (tid == 0) {
@@ -962,7 +989,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 #pragma unroll
         for (int cc = 0; cc < 2; ++cc) {
             const int j = jb + cc, pj = j - g.pad;
-            if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) in.accLr[(long long)blockIdx.y * g.nx_dom + pj] += glr[cc];
+            if (pj >= 0 && pj < g.nx_dom && j < g.nx - 1) in.accLr[(long long)(c.s0 / spg) * g.nx_dom + pj] += glr[cc];
         }
     }
 }
@@ -989,7 +1016,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     float4 *zt = xt + 4 * TX4;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::ADB);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const Ctx3 c = ctx4(g, spg, T::TZH, tiles_x);
+    const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordB, g.theavyB);
     const int nsh = c.s1 - c.s0;
     if (nsh <= 0) return;
     // the carry-in stresses of the exact gradient: one more box per shot from
@@ -1334,7 +1361,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                                                * (double)(ea[cc] + za[cc]);
                             const int pi = i - g.z0, pj = j - g.pad;
                             if (pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
-                                double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd +
+                                double *acc = o.acc + (long long)(c.s0 / spg) * o.accp * g.nd +
                                               (long long)pi * g.nx_dom + pj;
                                 atomicAdd(acc, glm);
                                 atomicAdd(acc + g.nd, glm);
@@ -1433,7 +1460,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 if (i < g.nz && j < g.nx && pi >= 0 && pi < g.nz_dom && pj >= 0 && pj < g.nx_dom) {
                     // one block per (tile, shot group) adds to these cells in a
                     // launch: the atomic adds only avoid waiting for the loads
-                    double *acc = o.acc + (long long)blockIdx.y * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
+                    double *acc = o.acc + (long long)(c.s0 / spg) * o.accp * g.nd + (long long)pi * g.nx_dom + pj;
                     if (EXACT) {
                         const double l2m = mL2M[r][cc], l = mL[r][cc];
                         const double id = 1.0 / ((l2m - l) * (l2m + l));

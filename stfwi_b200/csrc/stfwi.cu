@@ -67,6 +67,7 @@ struct stfwi_handle {
     int ntx = 1, ntza = 1, ntzb = 1;                       // tile counts
     int *tile_startA = nullptr, *tile_recA = nullptr;      // receivers grouped by the tw x tha tiles
     int *tile_startB = nullptr, *tile_recB = nullptr;      // receivers grouped by the tw x thb tiles
+    int *tordA = nullptr, *tordB = nullptr;                // tile dispatch orders, boundary tiles first
     int grp[4] = {1, 1, 1, 1}, spgk[4] = {1, 1, 1, 1};
     int acc_groups = 1, acc_used = 1;
     int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
@@ -811,6 +812,27 @@ void set_groups(stfwi_handle *h, const int spg_in[4])
 
 }  // namespace
 
+// tiles of a tw x th tiling in dispatch order, the `heavy` tiles first: those
+// whose own cells touch an edge margin, a C-PML strip or the free-surface
+// row, or whose staged box (one halo of K rows and 4 columns) reaches a strip
+// or the free-surface row, i.e. the tiles that take the guarded path
+std::vector<int> tile_order(const Geo &g, int K, int tw, int th, int ntx, int ntz, int *heavy)
+{
+    const int M = 2 * K + 1;
+    std::vector<int> hv, lt;
+    for (int t = 0; t < ntx * ntz; ++t) {
+        const int i0 = (t / ntx) * th, j0 = (t % ntx) * tw, i1 = i0 + th - 1, j1 = j0 + tw - 1;
+        bool plain = i0 >= M && i1 <= g.nz - 1 - M && j0 >= M && j1 <= g.nx - 1 - M && j0 >= g.pad &&
+                     j1 < g.nx - g.pad && i1 < g.nz - g.pad && (g.fs || i0 >= g.pad);
+        const int r0 = i0 - K, r1 = i1 + K, c0 = j0 - 4, c1 = j1 + 4;
+        const bool box = c0 < g.pad || c1 >= g.nx - g.pad || r1 >= g.nz - g.pad || r0 <= 0 || (!g.fs && r0 < g.pad);
+        (plain && !box ? lt : hv).push_back(t);
+    }
+    *heavy = (int)hv.size();
+    hv.insert(hv.end(), lt.begin(), lt.end());
+    return hv;
+}
+
 // ================================================================ C ABI
 
 
@@ -1082,6 +1104,7 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
           alloc((void **)&h->tile_startB, ((size_t)h->ntx * h->ntzb + 1) * 4) &&
           alloc((void **)&h->tile_recB, nrec * 4);
     ok &= alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
+    ok &= alloc((void **)&h->tordA, (size_t)h->ntx * h->ntza * 4) && alloc((void **)&h->tordB, (size_t)h->ntx * h->ntzb * 4);
     ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
     ok &= alloc((void **)&h->PX, (size_t)S * NPX * p.nz * p.xs_n * 4) &&
           alloc((void **)&h->PZ, (size_t)S * NPZ * p.zs_n * p.P * 4);
@@ -1115,6 +1138,18 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_CUDA;
     }
     cudaMemset(h->status, 0, 16);
+    {
+        const int K = d->fd_order / 2;
+        int ha = 0, hb = 0;
+        const std::vector<int> oa = tile_order(g, K, h->tw, h->tha, h->ntx, h->ntza, &ha);
+        const std::vector<int> ob = tile_order(g, K, h->tw, h->thb, h->ntx, h->ntzb, &hb);
+        if (cudaMemcpy(h->tordA, oa.data(), oa.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->tordB, ob.data(), ob.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+            stfwi_destroy(h);
+            return STFWI_ERR_CUDA;
+        }
+        g.tordA = h->tordA; g.tordB = h->tordB; g.theavyA = ha; g.theavyB = hb;
+    }
     // pitch padding and never-written cells read as zero by the tile copies
     cudaMemset(h->MATS, 0, (size_t)4 * NP * 4);
     cudaMemset(h->F, 0, (size_t)S * F_N * NP * 4);
@@ -1141,7 +1176,7 @@ void stfwi_destroy(stfwi_handle *h)
                     h->lm, h->rx, h->rz, h->F, h->A, h->PX, h->PZ, h->rec,
                     h->rec_adj, h->obs, h->snap, h->row0, h->acc, h->accLr, h->gtmp, h->energy,
                     h->mis_trace, h->mis_shot, h->src_a, h->pw, h->ptaper, h->pillum, h->ptmp, h->pscr, h->pmax,
-                    h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->CKF, h->CKPX,
+                    h->tile_startA, h->tile_recA, h->tile_startB, h->tile_recB, h->tordA, h->tordB, h->CKF, h->CKPX,
                     h->CKPZ};
     for (void *b : bufs)
         if (b) cudaFree(b);
