@@ -339,32 +339,6 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
             float *pSXX = px_ptr(g, PX, s, PX_SXX), *pSXZx = px_ptr(g, PX, s, PX_SXZ);
             float *pSXZz = pz_ptr(g, PZ, s, PZ_SXZ), *pSZZ = pz_ptr(g, PZ, s, PZ_SZZ);
-            // the C-PML memories of all the thread's cells, requested before
-            // any stencil (their latency overlaps instead of adding up per row)
-            float pxo[RPT][2][2], pzo[RPT][2][2], zbr[RPT], zar[RPT], zikr[RPT];
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = c.i0 + ty * RPT + r;
-                const int zs = i < g.nz ? zstrip_index(g, i) : -1;
-                zbr[r] = 0.f; zar[r] = 0.f; zikr[r] = 1.f;
-#pragma unroll
-                for (int cc = 0; cc < 2; ++cc) {
-                    const int j = jb + cc;
-                    pxo[r][cc][0] = pxo[r][cc][1] = pzo[r][cc][0] = pzo[r][cc][1] = 0.f;
-                    if (i >= g.nz - 1 || j < 1 || j >= g.nx - 1) continue;
-                    if (xs[cc] >= 0) {
-                        const int px = i * g.xs_n + xs[cc];
-                        pxo[r][cc][0] = pSXX[px];
-                        pxo[r][cc][1] = pSXZx[px];
-                    }
-                    if (zs >= 0) {
-                        const int pz = zs * g.P + j;
-                        pzo[r][cc][0] = pSXZz[pz];
-                        pzo[r][cc][1] = pSZZ[pz];
-                    }
-                }
-                if (zs >= 0 && i < g.nz - 1) { zbr[r] = m.bz[i]; zar[r] = m.az[i]; zikr[r] = m.ikz[i]; }
-            }
 #pragma unroll
             for (int r = 0; r < RPT; ++r) {
                 const int i = c.i0 + ty * RPT + r;
@@ -372,8 +346,28 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 float ax[10], az[10];
                 xrow(ax, sxx, q);
                 xrow(az, sxz, q);
-                const int zs = i < g.nz ? zstrip_index(g, i) : -1;
-                const float zb = zbr[r], za = zar[r], zik = zikr[r];
+                const int zs = zstrip_index(g, i);
+                // this row's C-PML memories, requested before the stencils
+                float pxo[2][2] = {{0.f, 0.f}, {0.f, 0.f}}, pzo[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+                float zb = 0.f, za = 0.f, zik = 1.f;
+                if (i < g.nz - 1) {
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc) {
+                        const int j = jb + cc;
+                        if (j < 1 || j >= g.nx - 1) continue;
+                        if (xs[cc] >= 0) {
+                            const int px = i * g.xs_n + xs[cc];
+                            pxo[cc][0] = pSXX[px];
+                            pxo[cc][1] = pSXZx[px];
+                        }
+                        if (zs >= 0) {
+                            const int pz = zs * g.P + j;
+                            pzo[cc][0] = pSXZz[pz];
+                            pzo[cc][1] = pSZZ[pz];
+                        }
+                    }
+                    if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
+                }
                 const float2 u2 = *reinterpret_cast<const float2 *>(own + (ty * RPT + r) * TX4 + 2 * tx);
                 const float2 v2 = *reinterpret_cast<const float2 *>(own + (T::TZH + ty * RPT + r) * TX4 + 2 * tx);
                 const float u[2] = {u2.x, u2.y}, v[2] = {v2.x, v2.y};
@@ -391,13 +385,13 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     float dzz = w_dp_t<FD>(wzz, r, cc, czp);
                     if (xs[cc] >= 0) {
                         const int px = i * g.xs_n + xs[cc];
-                        dxx = pml_fwd_pre(dxx, bxv[cc], axv[cc], ikxv[cc], pxo[r][cc][0], pSXX + px);
-                        dxxz = pml_fwd_pre(dxxz, bxv[cc], axv[cc], ikxv[cc], pxo[r][cc][1], pSXZx + px);
+                        dxx = pml_fwd_pre(dxx, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pSXX + px);
+                        dxxz = pml_fwd_pre(dxxz, bxv[cc], axv[cc], ikxv[cc], pxo[cc][1], pSXZx + px);
                     }
                     if (zs >= 0) {
                         const int pz = zs * g.P + j;
-                        dzxz = pml_fwd_pre(dzxz, zb, za, zik, pzo[r][cc][0], pSXZz + pz);
-                        dzz = pml_fwd_pre(dzz, zb, za, zik, pzo[r][cc][1], pSZZ + pz);
+                        dzxz = pml_fwd_pre(dzxz, zb, za, zik, pzo[cc][0], pSXZz + pz);
+                        dzz = pml_fwd_pre(dzz, zb, za, zik, pzo[cc][1], pSZZ + pz);
                     }
                     const float bxc = cc ? bx2[r].y : bx2[r].x, bzc = cc ? bz2[r].y : bz2[r].x;
                     un[cc] = u[cc] + bxc * dxx + bzc * dzxz;
@@ -582,32 +576,6 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int ssx = sh.sx[s], ssz = sh.sz[s], stype = sh.type[s];
             float *pDXU = px_ptr(g, PX, s, PX_DXU), *pDXV = px_ptr(g, PX, s, PX_DXV);
             float *pDZV = pz_ptr(g, PZ, s, PZ_DZV), *pDZU = pz_ptr(g, PZ, s, PZ_DZU);
-            // the C-PML memories of all the thread's cells, requested before
-            // any stencil (their latency overlaps instead of adding up per row)
-            float pxo[RPT][2][2], pzo[RPT][2][2], zbr[RPT], zar[RPT], zikr[RPT];
-#pragma unroll
-            for (int r = 0; r < RPT; ++r) {
-                const int i = c.i0 + ty * RPT + r;
-                const int zs = i < g.nz ? zstrip_index(g, i) : -1;
-                zbr[r] = 0.f; zar[r] = 0.f; zikr[r] = 1.f;
-#pragma unroll
-                for (int cc = 0; cc < 2; ++cc) {
-                    const int j = jb + cc;
-                    pxo[r][cc][0] = pxo[r][cc][1] = pzo[r][cc][0] = pzo[r][cc][1] = 0.f;
-                    if (i >= g.nz || j >= g.nx) continue;
-                    if (xs[cc] >= 0) {
-                        const int px = i * g.xs_n + xs[cc];
-                        if (j >= 1) pxo[r][cc][0] = pDXU[px];
-                        if (i < g.nz - 1) pxo[r][cc][1] = pDXV[px];
-                    }
-                    if (zs >= 0) {
-                        const int pz = zs * g.P + j;
-                        if (j < g.nx - 1) pzo[r][cc][0] = pDZV[pz];
-                        if (j >= 1) pzo[r][cc][1] = pDZU[pz];
-                    }
-                }
-                if (zs >= 0) { zbr[r] = m.bz[i]; zar[r] = m.az[i]; zikr[r] = m.ikz[i]; }
-            }
 #pragma unroll
             for (int r = 0; r < RPT; ++r) {
                 const int i = c.i0 + ty * RPT + r;
@@ -622,7 +590,25 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                 xrow(au, sU, q);
                 xrow(av, sV, q);
                 const int zs = zstrip_index(g, i);
-                const float zb = zbr[r], za = zar[r], zik = zikr[r];
+                // this row's C-PML memories, requested before the stencils
+                float pxo[2][2] = {{0.f, 0.f}, {0.f, 0.f}}, pzo[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+                float zb = 0.f, za = 0.f, zik = 1.f;
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const int j = jb + cc;
+                    if (j >= g.nx) continue;
+                    if (xs[cc] >= 0) {
+                        const int px = i * g.xs_n + xs[cc];
+                        if (j >= 1) pxo[cc][0] = pDXU[px];
+                        if (i < g.nz - 1) pxo[cc][1] = pDXV[px];
+                    }
+                    if (zs >= 0) {
+                        const int pz = zs * g.P + j;
+                        if (j < g.nx - 1) pzo[cc][0] = pDZV[pz];
+                        if (j >= 1) pzo[cc][1] = pDZU[pz];
+                    }
+                }
+                if (zs >= 0) { zb = m.bz[i]; za = m.az[i]; zik = m.ikz[i]; }
                 const float4 czm = zt[ty * RPT + r], czp = zt[T::TZH + ty * RPT + r];
                 float nxx[2], nzz[2], nxz[2];
 #pragma unroll
@@ -636,20 +622,20 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                     float dzu = w_dp_t<FD>(wU, r, cc, czp);
                     const int px = i * g.xs_n + xs[cc], pz = zs * g.P + j;
                     if (j >= 1 && xs[cc] >= 0)
-                        dxu = pml_fwd_pre(dxu, bxv[cc], axv[cc], ikxv[cc], pxo[r][cc][0], pDXU + px);
+                        dxu = pml_fwd_pre(dxu, bxv[cc], axv[cc], ikxv[cc], pxo[cc][0], pDXU + px);
                     if (j < g.nx - 1) {
                         if (g.fs && i == 0) dzv = Lr0[cc] * dxu * g.dzdx;
-                        if (zs >= 0) dzv = pml_fwd_pre(dzv, zb, za, zik, pzo[r][cc][0], pDZV + pz);
+                        if (zs >= 0) dzv = pml_fwd_pre(dzv, zb, za, zik, pzo[cc][0], pDZV + pz);
                     } else {
                         dzv = 0.f;
                     }
                     if (j >= 1) {
-                        if (zs >= 0) dzu = pml_fwd_pre(dzu, zb, za, zik, pzo[r][cc][1], pDZU + pz);
+                        if (zs >= 0) dzu = pml_fwd_pre(dzu, zb, za, zik, pzo[cc][1], pDZU + pz);
                     } else {
                         dzu = 0.f;
                     }
                     if (i < g.nz - 1) {
-                        if (xs[cc] >= 0) dxv = pml_fwd_pre(dxv, bxv[cc], axv[cc], ikxv[cc], pxo[r][cc][1], pDXV + px);
+                        if (xs[cc] >= 0) dxv = pml_fwd_pre(dxv, bxv[cc], axv[cc], ikxv[cc], pxo[cc][1], pDXV + px);
                     } else {
                         dxv = 0.f;
                     }
@@ -827,43 +813,30 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int *txs = reinterpret_cast<const int *>(tab + 4 * SW4);
             const float *tbz = tab + 5 * SW4, *taz = tbz + SH, *tikz = taz + SH;
             const int *tzs = reinterpret_cast<const int *>(tikz + SH);
-            // the C-PML memories of all the box rows this warp transforms,
-            // requested before any is used (one latency instead of one per row)
-            constexpr int NR = (SH + NWARP - 1) / NWARP;
-            float ps[NR][NCC][4];
-#pragma unroll
-            for (int t = 0; t < NR; ++t) {
-                const int rr = ty + t * NWARP;
-                const int i = c.i0 - K + rr;
-                const int zs = rr < SH ? tzs[rr] : -1;
-                // the C-PML memories of this row's cells, all requested before any is used
-#pragma unroll
-                for (int b = 0; b < NCC; ++b) {
-                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
-                    ps[t][b][0] = ps[t][b][1] = ps[t][b][2] = ps[t][b][3] = 0.f;
-                    if (cc >= SW4 || rr >= SH) continue;
-                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
-                        const long long pz = (long long)zs * g.P + jj;
-                        ps[t][b][0] = pDzV[pz];
-                        ps[t][b][1] = pDzU[pz];
-                    }
-                    const int xs = txs[cc];
-                    if (xs >= 0 && i >= 0 && i < g.nz) {
-                        const long long px = (long long)i * g.xs_n + xs;
-                        ps[t][b][2] = pDxU[px];
-                        ps[t][b][3] = pDxV[px];
-                    }
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < NR; ++t) {
-                const int rr = ty + t * NWARP;
-                if (rr >= SH) continue;
+            for (int rr = ty; rr < SH; rr += NWARP) {
                 const int i = c.i0 - K + rr;
                 const int zs = tzs[rr];
                 const bool rowsp = zs >= 0 || (g.fs && i == 0);
                 const bool own_row = rr >= K && rr < K + T::TZH;
                 // the C-PML memories of this row's cells, all requested before any is used
+                float ps[NCC][4];
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
+                    ps[b][0] = ps[b][1] = ps[b][2] = ps[b][3] = 0.f;
+                    if (cc >= SW4) continue;
+                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
+                        const long long pz = (long long)zs * g.P + jj;
+                        ps[b][0] = pDzV[pz];
+                        ps[b][1] = pDzU[pz];
+                    }
+                    const int xs = txs[cc];
+                    if (xs >= 0 && i >= 0 && i < g.nz) {
+                        const long long px = (long long)i * g.xs_n + xs;
+                        ps[b][2] = pDxU[px];
+                        ps[b][3] = pDxV[px];
+                    }
+                }
 #pragma unroll
                 for (int b = 0; b < NCC; ++b) {
                     const int cc = tx + b * TX;
@@ -881,16 +854,16 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                         const bool own = own_row && cc >= XO4 && cc < XO4 + TX4;
                         const int xs = txs[cc];
                         const long long pz = (long long)zs * g.P + jj, px = (long long)i * g.xs_n + xs;
-                        if (zs >= 0) vDzV = pml_adj4(za, tbz[rr], taz[rr], tikz[rr], ps[t][b][0], wDzV + pz, own);
+                        if (zs >= 0) vDzV = pml_adj4(za, tbz[rr], taz[rr], tikz[rr], ps[b][0], wDzV + pz, own);
                         float din = (jj >= 1) ? ea : 0.f;
                         if (g.fs && i == 0 && jj < g.nx - 1) din = tlr[cc] * vDzV + din;
                         vDxU = din;
-                        if (xs >= 0) vDxU = pml_adj4(din, tbx[cc], tax[cc], tikx[cc], ps[t][b][2], wDxU + px, own);
+                        if (xs >= 0) vDxU = pml_adj4(din, tbx[cc], tax[cc], tikx[cc], ps[b][2], wDxU + px, own);
                         const float h = (i < g.nz - 1 && jj < g.nx - 1) ? sa : 0.f;
                         vDzU = h;
                         vDxV = h;
-                        if (zs >= 0) vDzU = pml_adj4(h, tbz[rr], taz[rr], tikz[rr], ps[t][b][1], wDzU + pz, own);
-                        if (xs >= 0) vDxV = pml_adj4(h, tbx[cc], tax[cc], tikx[cc], ps[t][b][3], wDxV + px, own);
+                        if (zs >= 0) vDzU = pml_adj4(h, tbz[rr], taz[rr], tikz[rr], ps[b][1], wDzU + pz, own);
+                        if (xs >= 0) vDxV = pml_adj4(h, tbx[cc], tax[cc], tikx[cc], ps[b][3], wDxV + px, own);
                     }
                     S[q] = vDxU; S[SN + q] = vDzV; S[2 * SN + q] = vDzU; aDxV[q] = vDxV;
                 }
@@ -1128,41 +1101,29 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             const int *txs = reinterpret_cast<const int *>(tab + 4 * SW4);
             const float *tbz = tab + 5 * SW4, *taz = tbz + SH, *tikz = taz + SH;
             const int *tzs = reinterpret_cast<const int *>(tikz + SH);
-            // the C-PML memories of all the box rows this warp transforms,
-            // requested before any is used (one latency instead of one per row)
-            constexpr int NR = (SH + NWARP - 1) / NWARP;
-            float ps[NR][NCC][4];
-#pragma unroll
-            for (int t = 0; t < NR; ++t) {
-                const int rr = ty + t * NWARP;
-                const int i = c.i0 - K + rr;
-                const int zs = rr < SH ? tzs[rr] : -1;
-#pragma unroll
-                for (int b = 0; b < NCC; ++b) {
-                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
-                    ps[t][b][0] = ps[t][b][1] = ps[t][b][2] = ps[t][b][3] = 0.f;
-                    if (cc >= SW4 || rr >= SH) continue;
-                    const int xs = txs[cc];
-                    if (xs >= 0 && i >= 0 && i < g.nz) {
-                        const long long px = (long long)i * g.xs_n + xs;
-                        ps[t][b][0] = pXX[px];
-                        ps[t][b][1] = pXXZ[px];
-                    }
-                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
-                        const long long pz = (long long)zs * g.P + jj;
-                        ps[t][b][2] = pZXZ[pz];
-                        ps[t][b][3] = pZZ[pz];
-                    }
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < NR; ++t) {
-                const int rr = ty + t * NWARP;
-                if (rr >= SH) continue;
+            for (int rr = ty; rr < SH; rr += NWARP) {
                 const int i = c.i0 - K + rr;
                 const int zs = tzs[rr];
                 const bool rowsp = zs >= 0;
                 const bool own_row = rr >= K && rr < K + T::TZH;
+                float ps[NCC][4];
+#pragma unroll
+                for (int b = 0; b < NCC; ++b) {
+                    const int cc = tx + b * TX, jj = c.j0 - XO4 + cc;
+                    ps[b][0] = ps[b][1] = ps[b][2] = ps[b][3] = 0.f;
+                    if (cc >= SW4) continue;
+                    const int xs = txs[cc];
+                    if (xs >= 0 && i >= 0 && i < g.nz) {
+                        const long long px = (long long)i * g.xs_n + xs;
+                        ps[b][0] = pXX[px];
+                        ps[b][1] = pXXZ[px];
+                    }
+                    if (zs >= 0 && jj >= 0 && jj < g.nx) {
+                        const long long pz = (long long)zs * g.P + jj;
+                        ps[b][2] = pZXZ[pz];
+                        ps[b][3] = pZZ[pz];
+                    }
+                }
 #pragma unroll
                 for (int b = 0; b < NCC; ++b) {
                     const int cc = tx + b * TX;
@@ -1183,12 +1144,12 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
                         const int xs = txs[cc];
                         const long long px = (long long)i * g.xs_n + xs, pz = (long long)zs * g.P + jj;
                         if (xs >= 0) {
-                            vXX = pml_adj4(pv, tbx[cc], tax[cc], tikx[cc], ps[t][b][0], wXX + px, own);
-                            vXXZ = pml_adj4(qq, tbx[cc], tax[cc], tikx[cc], ps[t][b][1], wXXZ + px, own);
+                            vXX = pml_adj4(pv, tbx[cc], tax[cc], tikx[cc], ps[b][0], wXX + px, own);
+                            vXXZ = pml_adj4(qq, tbx[cc], tax[cc], tikx[cc], ps[b][1], wXXZ + px, own);
                         }
                         if (zs >= 0) {
-                            vZXZ = pml_adj4(pv, tbz[rr], taz[rr], tikz[rr], ps[t][b][2], wZXZ + pz, own);
-                            vZZ = pml_adj4(qq, tbz[rr], taz[rr], tikz[rr], ps[t][b][3], wZZ + pz, own);
+                            vZXZ = pml_adj4(pv, tbz[rr], taz[rr], tikz[rr], ps[b][2], wZXZ + pz, own);
+                            vZZ = pml_adj4(qq, tbz[rr], taz[rr], tikz[rr], ps[b][3], wZZ + pz, own);
                         }
                     }
                     S[q] = vXX; S[SN + q] = vZZ; aZXZ[q] = vZXZ; aXXZ[q] = vXXZ;
