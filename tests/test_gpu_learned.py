@@ -25,7 +25,12 @@ def test_learned_step_reaches_the_plain_error_sooner():
     for r in recs:
         print({k: r[k] for k in ("seed", "err_start", "target", "plain_time_s", "learned_time_s", "ratio",
                                  "learned_step_accepted", "err_after_learned_step")})
-    # the fallback keeps every model on track, and the learned method is faster overall
+    # the fallback keeps every model on track, and the learned method reaches
+    # the plain method's error in at most half its time (median over the four
+    # models; measured medians 0.28-0.43 on a B200)
+    import numpy as np
     assert all(r["learned_time_s"] is not None for r in recs)
     assert sum(bool(r["learned_step_accepted"]) for r in recs) >= 3
-    assert sum(r["learned_time_s"] for r in recs) < sum(r["plain_time_s"] for r in recs)
+    ratios = [r["ratio"] for r in recs]
+    print(f"learned / plain time: median {np.median(ratios):.2f}, per model {[round(x, 2) for x in ratios]}")
+    assert np.median(ratios) <= 0.5, ratios
