@@ -2,7 +2,7 @@
 custom grid: fd 8, free surface, 20-cell C-PML, seeded layered-fault model,
 shots every 7 cells alternating force and moment, receivers every 2 cells.
 
-    python benchmarks/probe_grid.py --nz 152 --nx 500 --shots 10 --variant 1
+    python benchmarks/probe_grid.py --nz 152 --nx 500 --shots 10
 """
 import argparse, os, sys, time
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -15,7 +15,6 @@ p.add_argument("--shots", type=int, default=10)
 p.add_argument("--nt", type=int, default=12)
 p.add_argument("--fd", type=int, default=8)
 p.add_argument("--reps", type=int, default=1)
-p.add_argument("--variant", type=int, default=0)
 a = p.parse_args()
 import torch
 from stfwi_b200 import Solver
@@ -28,7 +27,7 @@ rx = np.arange(0, a.nx, 2, dtype=np.int32); rz = np.ones_like(rx)
 wav = Mo.ricker(np.arange(a.nt) * 1.5e-3, 5.0, 0.3).astype(np.float32)
 torch.cuda.init()
 S = Solver(a.nz, a.nx, 20.0, 20.0, 1.5e-3, a.nt, 5.0, 20, len(rx), a.shots, fd_order=a.fd, free_surface=True,
-           want_gradient=True, kernel_variant=a.variant)
+           want_gradient=True)
 S.set_receivers(rx, rz); S.set_shots(sx, sz, types, wav); S.set_model(vs, vp, rho)
 obs = np.zeros((a.shots, a.nt, len(rx)), np.float32)
 for _ in range(a.reps):

@@ -19,7 +19,6 @@ def main():
     p.add_argument("--nt", type=int, default=40)
     p.add_argument("--reps", type=int, default=1)
     p.add_argument("--fd", type=int, default=8)
-    p.add_argument("--variant", type=int, default=0, help="kernel_variant of the handle")
     p.add_argument("--shot-group", type=int, default=0, help="shots per block (0: automatic)")
     a = p.parse_args()
     import torch
@@ -32,7 +31,7 @@ def main():
     torch.cuda.init()
     S = Solver(cfg["nz"], cfg["nx"], cfg["dx"], cfg["dz"], cfg["dt"], a.nt, cfg["fc"], cfg["pad"],
                len(rx), a.shots, fd_order=a.fd, free_surface=True, want_gradient=True,
-               kernel_variant=a.variant, shot_group=a.shot_group)
+               shot_group=a.shot_group)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav)
     S.set_model(vs, vp, rho)

@@ -64,11 +64,11 @@ typedef struct {
     double fc;              /* source peak frequency, used by the PML profile */
     int32_t want_gradient;  /* 1: reserve the stress history + accumulators (g_Vs, g_Vp);
                                2: also keep the velocities in the history, for the density
-                               gradient g_rho of both modes (kernel_variant 0 only) */
+                               gradient g_rho of both modes */
     int32_t shot_group;     /* shots per block (0: automatic) */
     double mem_budget_gb;   /* device memory the handle may use (0: 85% of free) */
-    int32_t kernel_variant; /* 0: two-column TMA-pipelined tiles (default), 1: plain shared-memory tiles,
-                               2: one-column TMA-pipelined tiles */
+    int32_t kernel_variant; /* must be 0 (the library has one stencil-kernel family; other values
+                               return STFWI_ERR_UNSUPPORTED) */
     int32_t ckpt_interval;  /* gradient history: 0 = keep every step if it fits the budget, else
                                checkpoint the state every k steps and recompute each k-step
                                segment during the adjoint (k chosen to fit); k > 0 = that k */

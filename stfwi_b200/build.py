@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libstfwi.so")
 SOURCES = [os.path.join(HERE, "csrc", "stfwi.cu"), os.path.join(HERE, "csrc", "nn.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "kernels_v4.cuh", "kernels_v5.cuh", "tma.cuh", "post.cuh", "umma.cuh")] \
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("common.cuh", "stencil_parts.cuh", "stencils.cuh", "tma.cuh", "post.cuh", "umma.cuh")] \
     + [os.path.join(ROOT, "include", f) for f in ("stfwi.h", "stfwi_nn.h")]
 
 NVCC_FLAGS = [

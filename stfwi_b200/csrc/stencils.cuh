@@ -1,8 +1,9 @@
 // Table-driven, pair-arithmetic stencil kernels (sm_100a).
 //
-// Same phases, state variables, tiling (64 x 16 tiles, two columns of two
-// rows per thread), TMA staging and per-term slice ranges as the two-column
-// kernels of kernels_v4.cuh, with two changes:
+// Four kernels per time step pair: fwd_vel (U, V), fwd_str (the stresses,
+// receivers, history), adj_a (P, Q) and adj_b (the strain adjoints and the
+// gradient sums), each over every tile of every shot of the batch, with the
+// tiling, TMA staging and per-term slice ranges of stencil_parts.cuh, and:
 //  * tiles that touch an edge, a C-PML strip or the free surface evaluate
 //    every stencil with per-column (x) and per-row (z) coefficient vectors
 //    from shared memory, the reference's dropped high-order terms as zero
@@ -16,7 +17,7 @@
 #pragma once
 #include <type_traits>
 
-#include "kernels_v4.cuh"
+#include "stencil_parts.cuh"
 
 namespace stfwi {
 
@@ -243,7 +244,7 @@ template <int FD> struct L5 {
 
 template <int FD>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
-    k5_fwd_vel(Geo g, Mat m, Shots sh, float *F, float *PX, float *PZ, int n, int spg, int tiles_x, int *status,
+    st_fwd_vel(Geo g, Mat m, Shots sh, float *F, float *PX, float *PZ, int n, int spg, int tiles_x, int *status,
                const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmUo)
 {
     using T = G4<FD, RPT4>;
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 template <int FD, bool ENERGY>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
-    k5_fwd_str(Geo g, Mat m, Shots sh, Recv rv, float *F, float *PX, float *PZ, int n, int spg, int tiles_x,
+    st_fwd_str(Geo g, Mat m, Shots sh, Recv rv, float *F, float *PX, float *PZ, int n, int spg, int tiles_x,
                FwdOut out, const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmSo)
 {
     using T = G4<FD, RPT4>;
@@ -729,7 +730,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 template <int FD>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
-    k5_adj_a(Geo g, Mat m, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x, AdjIn in,
+    st_adj_a(Geo g, Mat m, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x, AdjIn in,
              int *status, const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmPQo)
 {
     using T = G4<FD, RPT4>;
@@ -971,7 +972,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 template <int FD, bool EXACT, bool IMG, bool RHO>
 __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
-    k5_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
+    st_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
              AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ,
              const __grid_constant__ CUtensorMap tmEo, const __grid_constant__ CUtensorMap tmH)
 {

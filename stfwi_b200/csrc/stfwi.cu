@@ -16,8 +16,7 @@
 #include <vector>
 
 #include "../../include/stfwi.h"
-#include "kernels_v4.cuh"
-#include "kernels_v5.cuh"
+#include "stencils.cuh"
 #include "post.cuh"
 
 using namespace stfwi;
@@ -55,7 +54,6 @@ struct stfwi_handle {
     bool model_set = false;
     // tensor maps of the staged tiles and per-kernel shot groups
     int sms = 148;
-    int kv = 0;     // kernel family: 0 two-column tiles, 1 table-driven paired tiles
     int accp = 5;   // accumulator planes per shot group (7 with the density terms)
     CUtensorMap tmS{}, tmV{}, tmE{}, tmPQ{};
     CUtensorMap tmUo{}, tmSo{}, tmPQo{}, tmEo{};   // own-cell boxes of the two-column kernels
@@ -424,48 +422,31 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
 }
 
 template <int FD>
-void launch_fwd_step_v5(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
     const int tiles = h->ntx * h->ntza;
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     prof_mark(h, 0, n, 0, st);
-    k5_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L5<FD>::bytes(L5<FD>::VEL, 2), st>>>(
+    st_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L5<FD>::bytes(L5<FD>::VEL, 2), st>>>(
         h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
-    auto str = o.energy ? k5_fwd_str<FD, true> : k5_fwd_str<FD, false>;
+    auto str = o.energy ? st_fwd_str<FD, true> : st_fwd_str<FD, false>;
     str<<<dim3(tiles, h->grp[1]), block, L5<FD>::bytes(L5<FD>::STR, 2), st>>>(
         h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
     prof_mark(h, 1, n, 1, st);
 }
 
-template <int FD>
-void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
-{
-    if (h->kv == 1) return launch_fwd_step_v5<FD>(h, n, o, st);
-    const int tiles = h->ntx * h->ntza;
-    dim3 block(TX, NWARP);
-    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    prof_mark(h, 0, n, 0, st);
-    k4_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L4<FD>::bytes(L4<FD>::VEL, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
-    prof_mark(h, 0, n, 1, st);
-    prof_mark(h, 1, n, 0, st);
-    auto str = o.energy ? k4_fwd_str<FD, true> : k4_fwd_str<FD, false>;
-    str<<<dim3(tiles, h->grp[1]), block, L4<FD>::bytes(L4<FD>::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
-    prof_mark(h, 1, n, 1, st);
-}
 
 template <int FD>
-void launch_adj_step_v5(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
 {
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
     prof_mark(h, 2, n, 0, st);
-    k5_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L5<FD>::bytes(L5<FD>::ADA, 2), st>>>(
+    st_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L5<FD>::bytes(L5<FD>::ADA, 2), st>>>(
         h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
     prof_mark(h, 2, n, 1, st);
     prof_mark(h, 3, n, 0, st);
@@ -475,37 +456,13 @@ void launch_adj_step_v5(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &a
             h->tmPQ, h->tmEo, h->tmH);
     };
     const bool rho = h->g.snf == 5;
-    if (ao.want_exact && ao.want_img) rho ? launch(k5_adj_b<FD, true, true, true>) : launch(k5_adj_b<FD, true, true, false>);
-    else if (ao.want_exact) rho ? launch(k5_adj_b<FD, true, false, true>) : launch(k5_adj_b<FD, true, false, false>);
-    else if (ao.want_img) rho ? launch(k5_adj_b<FD, false, true, true>) : launch(k5_adj_b<FD, false, true, false>);
-    else launch(k5_adj_b<FD, false, false, false>);
+    if (ao.want_exact && ao.want_img) rho ? launch(st_adj_b<FD, true, true, true>) : launch(st_adj_b<FD, true, true, false>);
+    else if (ao.want_exact) rho ? launch(st_adj_b<FD, true, false, true>) : launch(st_adj_b<FD, true, false, false>);
+    else if (ao.want_img) rho ? launch(st_adj_b<FD, false, true, true>) : launch(st_adj_b<FD, false, true, false>);
+    else launch(st_adj_b<FD, false, false, false>);
     prof_mark(h, 3, n, 1, st);
 }
 
-template <int FD>
-void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
-{
-    if (h->kv == 1) return launch_adj_step_v5<FD>(h, n, ai, ao, st);
-    dim3 block(TX, NWARP);
-    Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
-    prof_mark(h, 2, n, 0, st);
-    k4_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L4<FD>::bytes(L4<FD>::ADA, 2), st>>>(
-        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
-    prof_mark(h, 2, n, 1, st);
-    prof_mark(h, 3, n, 0, st);
-    auto launch = [&](auto kern) {
-        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L4<FD>::bytes(L4<FD>::ADB, 2), st>>>(
-            h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
-            h->tmPQ, h->tmEo, h->tmH);
-    };
-    const bool rho = h->g.snf == 5;
-    if (ao.want_exact && ao.want_img) rho ? launch(k4_adj_b<FD, true, true, true>) : launch(k4_adj_b<FD, true, true, false>);
-    else if (ao.want_exact) rho ? launch(k4_adj_b<FD, true, false, true>) : launch(k4_adj_b<FD, true, false, false>);
-    else if (ao.want_img) rho ? launch(k4_adj_b<FD, false, true, true>) : launch(k4_adj_b<FD, false, true, false>);
-    else launch(k4_adj_b<FD, false, false, false>);
-    prof_mark(h, 3, n, 1, st);
-}
 
 stfwi_status zero_forward_state(stfwi_handle *h, cudaStream_t st)
 {
@@ -721,38 +678,22 @@ stfwi_status set_smem(stfwi_handle *h, const void *const (&kern)[7])
 template <int FD>
 stfwi_status setup_tma_kernels(stfwi_handle *h)
 {
-    if (h->kv == 1) {
-        const void *const kern[7] = {
-            (const void *)k5_fwd_vel<FD>, (const void *)k5_fwd_str<FD, false>, (const void *)k5_adj_a<FD>,
-            (const void *)k5_adj_b<FD, true, false, false>, (const void *)k5_adj_b<FD, true, true, false>,
-            (const void *)k5_adj_b<FD, false, true, false>, (const void *)k5_adj_b<FD, false, false, false>};
-        stfwi_status r = set_smem<L5<FD>>(h, kern);
-        if (r) return r;
-        CK(h, cudaFuncSetAttribute((const void *)k5_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)L5<FD>::bytes(L5<FD>::STR, 2)));
-        const void *const rho_kern[3] = {(const void *)k5_adj_b<FD, true, false, true>,
-                                         (const void *)k5_adj_b<FD, true, true, true>,
-                                         (const void *)k5_adj_b<FD, false, true, true>};
-        for (const void *k : rho_kern)
-            CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)L5<FD>::bytes(L5<FD>::ADB, 2)));
-        return STFWI_OK;
-    }
     const void *const kern[7] = {
-        (const void *)k4_fwd_vel<FD>, (const void *)k4_fwd_str<FD, false>, (const void *)k4_adj_a<FD>,
-        (const void *)k4_adj_b<FD, true, false, false>, (const void *)k4_adj_b<FD, true, true, false>,
-        (const void *)k4_adj_b<FD, false, true, false>, (const void *)k4_adj_b<FD, false, false, false>};
-    stfwi_status r = set_smem<L4<FD>>(h, kern);
+        (const void *)st_fwd_vel<FD>, (const void *)st_fwd_str<FD, false>, (const void *)st_adj_a<FD>,
+        (const void *)st_adj_b<FD, true, false, false>, (const void *)st_adj_b<FD, true, true, false>,
+        (const void *)st_adj_b<FD, false, true, false>, (const void *)st_adj_b<FD, false, false, false>};
+    stfwi_status r = set_smem<L5<FD>>(h, kern);
     if (r) return r;
-    CK(h, cudaFuncSetAttribute((const void *)k4_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)L4<FD>::bytes(L4<FD>::STR, 2)));
-    // the density-gradient instantiations of the strain phase
-    const void *const rho_kern[3] = {(const void *)k4_adj_b<FD, true, false, true>,
-                                     (const void *)k4_adj_b<FD, true, true, true>,
-                                     (const void *)k4_adj_b<FD, false, true, true>};
+    CK(h, cudaFuncSetAttribute((const void *)st_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)L5<FD>::bytes(L5<FD>::STR, 2)));
+    const void *const rho_kern[3] = {(const void *)st_adj_b<FD, true, false, true>,
+                                     (const void *)st_adj_b<FD, true, true, true>,
+                                     (const void *)st_adj_b<FD, false, true, true>};
     for (const void *k : rho_kern)
-        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L4<FD>::bytes(L4<FD>::ADB, 2)));
+        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)L5<FD>::bytes(L5<FD>::ADB, 2)));
     return STFWI_OK;
+
 }
 
 stfwi_status setup_tensor_maps(stfwi_handle *h)
@@ -1010,7 +951,8 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     if (!d || !out) return STFWI_ERR_INVALID;
     *out = nullptr;
     if (d->fd_order != 2 && d->fd_order != 4 && d->fd_order != 8) return STFWI_ERR_UNSUPPORTED;
-    if (d->kernel_variant != 0 && d->kernel_variant != 1) return STFWI_ERR_UNSUPPORTED;
+    // one kernel family: the field is kept for the ABI, other values are refused
+    if (d->kernel_variant != 0) return STFWI_ERR_UNSUPPORTED;
     if (d->want_gradient < 0 || d->want_gradient > 2) return STFWI_ERR_INVALID;
     const int H = d->fd_order / 2;
     if (d->nz_dom < 1 || d->nx_dom < 1 || d->pad < H || d->nt < 1 || d->nrec < 0 || d->max_shots < 1 ||
@@ -1063,7 +1005,6 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.wait_polls = WAIT3;
     h->accp = g.snf == 5 ? 7 : 5;
     h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
-    h->kv = d->kernel_variant;
     h->ntx = (int)((p.nx + h->tw - 1) / h->tw);
     h->ntza = (int)((p.nz + h->tha - 1) / h->tha);
     h->ntzb = (int)((p.nz + h->thb - 1) / h->thb);

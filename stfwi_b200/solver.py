@@ -72,8 +72,7 @@ class Solver:
         h = ct.c_void_p()
         st = self.lib.stfwi_create(ct.byref(self.desc), ct.byref(h))
         if st == N.STFWI_ERR_UNSUPPORTED:
-            raise NotImplementedError(f"stfwi_create: unsupported configuration {self.shape_desc()}"
-                                      + (" (the density gradient needs kernel_variant 0)" if density else ""))
+            raise NotImplementedError(f"stfwi_create: unsupported configuration {self.shape_desc()}")
         if st == N.STFWI_ERR_INVALID:
             raise ValueError(f"stfwi_create: invalid descriptor {self.shape_desc()}")
         if st != N.STFWI_OK:

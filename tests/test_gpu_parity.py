@@ -29,19 +29,17 @@ def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx
                   want_gradient=want_gradient, **kw)
 
 
-VARIANTS = [0, 1]  # kernel families: two-column tiles, table-driven paired tiles (stfwi_desc.kernel_variant)
 
 
-@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("fd,fs,st", C.CONFIGS)
-def test_forward_and_adjoint_vs_oracle(fd, fs, st, variant):
+def test_forward_and_adjoint_vs_oracle(fd, fs, st):
     """The reference's dot-product case (test_adjoint_kernel.py) on the GPU:
     seismograms and the source adjoint against the FP64 oracle, and the
     dot-product identity of the FP32 kernels."""
     vs, vp, rho = C.model()
     sx, sz, rx, rz = C.acquisition(fs, st)
     s_in, ys = C.random_vectors()
-    S = _solver(C.NT, len(rx), 1, fd, fs, kernel_variant=variant)
+    S = _solver(C.NT, len(rx), 1, fd, fs)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots([sx], [sz], [st], s_in.astype(np.float32))
@@ -62,10 +60,9 @@ def test_forward_and_adjoint_vs_oracle(fd, fs, st, variant):
     S.close()
 
 
-@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("fd,fs,st", [(8, True, "force"), (8, True, "moment"), (4, False, "force"),
                                       (2, False, "moment")])
-def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st, variant):
+def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st):
     """Model gradients of the GPU (FP32 stencils, FP64 sums) against the
     FP64 oracle on a small case: exact (AD) and imaging formula."""
     vs, vp, rho = C.model()
@@ -79,7 +76,7 @@ def test_exact_and_imaging_gradient_vs_oracle(fd, fs, st, variant):
               scale=1.0, invert="vs_vp", **geo)
     (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
     (gi_vs, gi_vp, _), _ = O.compute_gradient("adjoint", Vs=vs, Vp=vp, rho=rho, **kw)
-    S = _solver(nt, len(rx), 1, fd, fs, want_gradient=True, kernel_variant=variant)
+    S = _solver(nt, len(rx), 1, fd, fs, want_gradient=True)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots([sx], [sz], [st], wav.astype(np.float32))
@@ -133,8 +130,7 @@ def test_marmousi_known_answers(known_answers):
     S.close()
 
 
-@pytest.mark.parametrize("variant", VARIANTS)
-def test_batch_of_shots_matches_single_shots(variant):
+def test_batch_of_shots_matches_single_shots():
     """A batch of 7 mixed force/moment shots (several shots per block, both
     pipeline stages in use) gives each shot's traces and the summed gradient
     of the single-shot runs."""
@@ -148,7 +144,7 @@ def test_batch_of_shots_matches_single_shots(variant):
     wav = (O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9).astype(np.float32)
     rng = np.random.default_rng(5)
     obs = rng.standard_normal((7, nt, len(rx))).astype(np.float32) * 1e-9
-    S = _solver(nt, len(rx), 7, fd, fs, want_gradient=True, kernel_variant=variant, shot_group=2)
+    S = _solver(nt, len(rx), 7, fd, fs, want_gradient=True, shot_group=2)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav)
@@ -159,7 +155,7 @@ def test_batch_of_shots_matches_single_shots(variant):
     S.close()
     gsum = np.zeros_like(g)
     for k in range(7):
-        S1 = _solver(nt, len(rx), 1, fd, fs, want_gradient=True, kernel_variant=variant)
+        S1 = _solver(nt, len(rx), 1, fd, fs, want_gradient=True)
         S1.set_model(vs, vp, rho)
         S1.set_receivers(rx, rz)
         S1.set_shots(sx[k:k + 1], sz[k:k + 1], types[k:k + 1], wav)
@@ -173,8 +169,7 @@ def test_batch_of_shots_matches_single_shots(variant):
     assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
 
 
-@pytest.mark.parametrize("variant", VARIANTS)
-def test_checkpointed_gradient_equals_store_all(variant):
+def test_checkpointed_gradient_equals_store_all():
     """Checkpoint every k steps + recompute gives the gradient of the
     every-step history (the recompute is deterministic), for an explicit k
     that does not divide nt and for the k a small memory budget forces."""
@@ -187,7 +182,7 @@ def test_checkpointed_gradient_equals_store_all(variant):
     obs = np.random.default_rng(3).standard_normal((2, nt, len(rx))).astype(np.float32) * 1e-9
     out = []
     for ck, budget in ((0, 0.0), (7, 0.0), (0, 0.06)):
-        S = _solver(nt, len(rx), 2, fd, fs, want_gradient=True, kernel_variant=variant, ckpt_interval=ck,
+        S = _solver(nt, len(rx), 2, fd, fs, want_gradient=True, ckpt_interval=ck,
                     mem_budget_gb=budget)
         S.set_model(vs, vp, rho)
         S.set_receivers(rx, rz)
@@ -216,9 +211,8 @@ def _smooth_model(nz, nx, seed):
     return vs, vp, rho
 
 
-@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("fd,fs", [(8, True), (8, False), (4, True), (2, False)])
-def test_multi_tile_grid_vs_oracle(fd, fs, variant):
+def test_multi_tile_grid_vs_oracle(fd, fs):
     """A grid of several tiles in x and z (interior tiles without the C-PML
     fix-up, tile edges inside the stencil reach), with sources and receivers
     near tile edges: seismograms, misfit and the exact gradient against the
@@ -244,7 +238,7 @@ def test_multi_tile_grid_vs_oracle(fd, fs, variant):
               scale=1.0, invert="vs_vp", **geo)
     (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
     S = _solver(nt, len(rx), 3, fd, fs, want_gradient=True, pad=pad, nz=nz, nx=nx, dx=dx, dz=dz, dt=dt,
-                fc=fc, kernel_variant=variant)
+                fc=fc)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav.astype(np.float32))
@@ -258,7 +252,7 @@ def test_multi_tile_grid_vs_oracle(fd, fs, variant):
     g = S.gradient(exact=True)
     errs = {"misfit": abs(mis.sum() / loss - 1), "exact_vs": _rel(g["exact"][0], gx_vs),
             "exact_vp": _rel(g["exact"][1], gx_vp)}
-    print(f"multi-tile fd{fd} fs={fs} variant {variant}: amplification {amp:.1f} errors {errs}")
+    print(f"multi-tile fd{fd} fs={fs}: amplification {amp:.1f} errors {errs}")
     tol = 2e-5 * max(amp, 1.0)
     assert all(e < tol for e in errs.values()), (tol, errs)
     S.close()
