@@ -159,7 +159,7 @@ def cpu_gradient_rate(cfg, nshot, nt, threads=None, precision=32, ckpt=25):
     return nshot * cells * nt / dt / 1e9, dt
 
 
-def cpu_sample(cfg, ncores, nt=200):
+def cpu_sample(cfg, ncores, nt=500):
     """Shots and steps of the CPU sample: one shot per core, and a step count
     whose store-all history (16 FP32 fields per cell and step) stays within a
     third of the host's free memory."""
@@ -277,8 +277,10 @@ def main():
     sos = butter(6, 3.0, fs=1.0 / cfg["dt"], output="sos")
     n_taper = int(0.1 * nt)
     S.set_model(vs0, vp0, rho0)
-    # shots per block of each kernel, timed on this workload (untimed set-up)
+    # tile shapes and shots per block of each kernel, timed on this workload
+    # (untimed set-up)
     schedule = None if args.no_autotune else S.autotune(steps=20)
+    tile_rows = dict(zip(("fwd_vel,fwd_str,adj_a", "adj_b"), S.tile_rows()))
     mis_d = torch.zeros(ns, dtype=torch.float64, device="cuda")
     g_d = torch.zeros((1, 3, cfg["nz"], cfg["nx"]), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
@@ -423,7 +425,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(config_json(cfg, world), shots_per_block=schedule), "roofline": roof,
+                "config": dict(config_json(cfg, world), shots_per_block=schedule, tile_rows=tile_rows,
+                              tile_cols=64), "roofline": roof,
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h)},

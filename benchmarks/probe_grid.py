@@ -15,6 +15,8 @@ p.add_argument("--shots", type=int, default=10)
 p.add_argument("--nt", type=int, default=12)
 p.add_argument("--fd", type=int, default=8)
 p.add_argument("--reps", type=int, default=1)
+p.add_argument("--tile-rows", type=int, nargs=2, default=None, metavar=("A", "B"),
+               help="tile heights (8 or 16) of fwd_vel/fwd_str/adj_a and of adj_b; default: autotune")
 a = p.parse_args()
 import torch
 from stfwi_b200 import Solver
@@ -29,6 +31,11 @@ torch.cuda.init()
 S = Solver(a.nz, a.nx, 20.0, 20.0, 1.5e-3, a.nt, 5.0, 20, len(rx), a.shots, fd_order=a.fd, free_surface=True,
            want_gradient=True)
 S.set_receivers(rx, rz); S.set_shots(sx, sz, types, wav); S.set_model(vs, vp, rho)
+if a.tile_rows:
+    S.set_tile_rows(*a.tile_rows)
+    print("tile rows", S.tile_rows())
+else:
+    print("autotuned: shots per block", S.autotune(steps=20), "tile rows", S.tile_rows())
 obs = np.zeros((a.shots, a.nt, len(rx)), np.float32)
 for _ in range(a.reps):
     t0 = time.perf_counter()

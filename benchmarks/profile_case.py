@@ -20,6 +20,8 @@ def main():
     p.add_argument("--reps", type=int, default=1)
     p.add_argument("--fd", type=int, default=8)
     p.add_argument("--shot-group", type=int, default=0, help="shots per block (0: automatic)")
+    p.add_argument("--tile-rows", type=int, nargs=2, default=(16, 16), metavar=("A", "B"),
+                   help="tile heights of fwd_vel/fwd_str/adj_a and of adj_b (8 or 16)")
     a = p.parse_args()
     import torch
     from stfwi_b200 import Solver
@@ -35,6 +37,7 @@ def main():
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav)
     S.set_model(vs, vp, rho)
+    S.set_tile_rows(*a.tile_rows)
     obs = np.zeros((a.shots, a.nt, len(rx)), np.float32)
     for _ in range(a.reps):
         t0 = time.perf_counter()

@@ -171,14 +171,24 @@ stfwi_status stfwi_profile(stfwi_handle *h, int32_t every);
 stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out);
 
 /* Tile-schedule autotuner (no counterpart in the reference): times `steps`
- * forward and adjoint steps of the handle's configuration for several
- * numbers of shots per block (1-8) with CUDA events around every kernel,
- * and keeps the fastest for each of the four stencil kernels (also across
- * later stfwi_set_shots calls); spg_out [4] (optional) receives the choice
- * for fwd_vel, fwd_str, adj_a, adj_b.  Overwrites the fields and history:
- * call it before the forward whose history a gradient will use.  A
- * descriptor shot_group > 0 overrides the result.  Kernel variants 0, 2. */
+ * forward and adjoint steps of the handle's configuration for both tile
+ * shapes (64 x 8 and 64 x 16 cells) and several numbers of shots per block
+ * (1-25) with CUDA events around every kernel, and keeps the fastest: one
+ * tile shape for fwd_vel, fwd_str and adj_a (they share the receivers' tile
+ * lists), one for adj_b, and the shots per block of each of the four
+ * stencil kernels (also across later stfwi_set_shots calls); spg_out [4]
+ * (optional) receives the shots per block of fwd_vel, fwd_str, adj_a, adj_b,
+ * stfwi_tile_rows the tile shapes.  Overwrites the fields and history: call
+ * it before the forward whose history a gradient will use.  A descriptor
+ * shot_group > 0 overrides the shots per block. */
 stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, void *stream);
+
+/* Tile heights in rows (8 or 16; 16 and 16 until the autotuner has run):
+ * rows_a for fwd_vel, fwd_str and adj_a, rows_b for adj_b.  Any other value
+ * is STFWI_ERR_INVALID.  The fields and a kept history stay valid. */
+stfwi_status stfwi_set_tile_rows(stfwi_handle *h, int32_t rows_a, int32_t rows_b);
+/* rows_out [2]: the tile heights in use (rows_a, rows_b). */
+stfwi_status stfwi_tile_rows(const stfwi_handle *h, int32_t *rows_out);
 
 /* Residual preparation that allocates nothing (no counterpart in the
  * reference): the same misfit and adjoint sources as stfwi_misfit, without a

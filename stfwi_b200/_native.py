@@ -28,6 +28,7 @@ EXPORTS = (
     "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
     "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
     "stfwi_forward_frames", "stfwi_adjoint_frames", "stfwi_imaging_condition", "stfwi_set_wait_limit",
+    "stfwi_set_tile_rows", "stfwi_tile_rows",
 )
 
 # full wavefield frames (bit set, in this order)
@@ -119,6 +120,8 @@ def load():
         L.stfwi_autotune.argtypes = [H, i32, vp, vp]
         L.stfwi_forward_frames.argtypes = [H, u32, vp, vp]
         L.stfwi_set_wait_limit.argtypes = [H, ct.c_int64]
+        L.stfwi_set_tile_rows.argtypes = [H, i32, i32]
+        L.stfwi_tile_rows.argtypes = [H, vp]
         L.stfwi_adjoint_frames.argtypes = [H, u32, vp, vp, vp]
         L.stfwi_imaging_condition.argtypes = [ct.POINTER(StfwiImagingDesc)] + [vp] * 10 + [vp, vp]
         sz, f32 = ct.c_size_t, ct.c_float

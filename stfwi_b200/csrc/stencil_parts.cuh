@@ -16,8 +16,8 @@
 
 namespace stfwi {
 
-#ifndef STFWI_V4_MINBLOCKS
-#define STFWI_V4_MINBLOCKS 2
+#ifndef STFWI_MINBLOCKS
+#define STFWI_MINBLOCKS 2
 #endif
 
 constexpr int TX4 = 64;               // tile width: 32 lanes x 2 columns
@@ -34,18 +34,16 @@ template <int FD, int RPT> struct G4 {
     static constexpr int S1 = al32_3(SN), S2 = al32_3(2 * SN), S3 = al32_3(3 * SN);
 };
 
-#ifndef STFWI_V4_RPT
-#define STFWI_V4_RPT 2
-#endif
-#ifndef STFWI_V4_RPTB
-#define STFWI_V4_RPTB 2
-#endif
-constexpr int RPT4 = STFWI_V4_RPT;    // rows per thread: fwd_vel, fwd_str, adj_a
-constexpr int RPT4B = STFWI_V4_RPTB;  // rows per thread: adj_b (FP64 sums per cell in registers)
+// rows per thread: every kernel is built for 1 and 2 (8- and 16-row tiles);
+// a handle runs fwd_vel, fwd_str and adj_a on one tile height and adj_b on
+// another, chosen by the autotuner (2 and 2 until it has run)
+constexpr int RPT_MIN = 1, RPT_DEFAULT = 2;
 
-template <int FD> struct L4 {
-    using A = G4<FD, RPT4>;
-    using B = G4<FD, RPT4B>;
+// shared-memory plan of R rows per thread; the velocity, stress and adj_a
+// kernels use the A-layout members, adj_b the B-layout ones
+template <int FD, int R> struct L4 {
+    using A = G4<FD, R>;
+    using B = G4<FD, R>;
     // own-cell boxes (no halo) staged beside the halo boxes: U, V for the
     // velocity phase, sxx, szz, sxz for the stress phase
     static constexpr int OWN2 = al32_3(2 * A::TZH * TX4), OWN3 = al32_3(3 * A::TZH * TX4);

@@ -230,8 +230,8 @@ __device__ __forceinline__ Ctx3 ctx5(const Geo &g, int spg, int tzh, int tiles_x
 // shared-memory plans of the table-driven kernels: the two-column layout
 // followed by the coefficient tables (float4 per column of the tile for
 // each x-stencil set, per row of the tile for each z-stencil set)
-template <int FD> struct L5 {
-    using P4 = L4<FD>;
+template <int FD, int R> struct L5 {
+    using P4 = L4<FD, R>;
     static constexpr int CTA = 4 * (2 * TX4 + 2 * P4::A::TZH);                    // 2 x-sets, 2 z-sets
     static constexpr int CTB = 4 * (4 * TX4 + 4 * P4::A::TZH);                    // 4 x-sets, 4 z-sets (adj_a)
     static constexpr int CTBB = 4 * (4 * TX4 + 4 * P4::B::TZH);                   // 4 x-sets, 4 z-sets (adj_b)
@@ -242,19 +242,19 @@ template <int FD> struct L5 {
 
 // ------------------------------------------------------------- forward: velocities
 
-template <int FD>
-__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+template <int FD, int RPT>
+__global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
     st_fwd_vel(Geo g, Mat m, Shots sh, float *F, float *PX, float *PZ, int n, int spg, int tiles_x, int *status,
                const __grid_constant__ CUtensorMap tmS, const __grid_constant__ CUtensorMap tmUo)
 {
-    using T = G4<FD, RPT4>;
-    constexpr int K = T::K, SN = T::SN, RPT = RPT4;
-    constexpr int STG = L4<FD>::VEL_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
+    using T = G4<FD, RPT>;
+    constexpr int K = T::K, SN = T::SN;
+    constexpr int STG = L4<FD, RPT>::VEL_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     // coefficient tables: x sets (D+ of sxx, D- of sxz), z sets (D- of sxz, D+ of szz)
-    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD>::VEL);
+    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD, RPT>::VEL);
     float4 *zt = xt + 2 * TX4;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::VEL);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD, RPT>::VEL);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
@@ -425,19 +425,19 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 // ------------------------------------------------------------- forward: stresses
 
-template <int FD, bool ENERGY>
-__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+template <int FD, int RPT, bool ENERGY>
+__global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
     st_fwd_str(Geo g, Mat m, Shots sh, Recv rv, float *F, float *PX, float *PZ, int n, int spg, int tiles_x,
                FwdOut out, const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmSo)
 {
-    using T = G4<FD, RPT4>;
-    constexpr int K = T::K, SN = T::SN, RPT = RPT4;
-    constexpr int STG = L4<FD>::STR_STAGE, OWNB = 3 * T::TZH * TX4 * 4;
+    using T = G4<FD, RPT>;
+    constexpr int K = T::K, SN = T::SN;
+    constexpr int STG = L4<FD, RPT>::STR_STAGE, OWNB = 3 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     // coefficient tables: x sets (D- of U, D+ of V), z sets (D- of V, D+ of U)
-    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD>::STR);
+    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD, RPT>::STR);
     float4 *zt = xt + 2 * TX4;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::STR);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD, RPT>::STR);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
@@ -728,14 +728,14 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 // ------------------------------------------------------------- adjoint: P = B U_a, Q = B V_a
 
-template <int FD>
-__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+template <int FD, int RPT>
+__global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
     st_adj_a(Geo g, Mat m, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x, AdjIn in,
              int *status, const __grid_constant__ CUtensorMap tmE, const __grid_constant__ CUtensorMap tmPQo)
 {
-    using T = G4<FD, RPT4>;
-    constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4;
-    constexpr int STG = L4<FD>::ADA_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
+    using T = G4<FD, RPT>;
+    constexpr int K = T::K, SN = T::SN, SH = T::SH;
+    constexpr int STG = L4<FD, RPT>::ADA_STAGE, OWNB = 2 * T::TZH * TX4 * 4;
     extern __shared__ __align__(128) float sm[];
     constexpr int NCC = (SW4 + TX - 1) / TX;
     float *aDxV = sm + 2 * STG;
@@ -743,9 +743,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     // coefficient tables: x sets (A, B of the transposed D- of exx_a, A, B of
     // the transposed D+ of exz_a), z sets (A, B of the transposed D+ of exz_a,
     // A, B of the transposed D- of ezz_a)
-    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD>::ADA);
+    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD, RPT>::ADA);
     float4 *zt = xt + 4 * TX4;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::ADA);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD, RPT>::ADA);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordA, g.theavyA);
     const int nsh = c.s1 - c.s0;
@@ -970,15 +970,15 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
 
 // ------------------------------------------------------------- adjoint: strains + gradient
 
-template <int FD, bool EXACT, bool IMG, bool RHO>
-__global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
+template <int FD, int RPT, bool EXACT, bool IMG, bool RHO>
+__global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
     st_adj_b(Geo g, Mat m, Shots sh, Recv rv, float *A, float *PX, float *PZ, int n, int spg, int tiles_x,
              AdjOut o, int *status, const __grid_constant__ CUtensorMap tmPQ,
              const __grid_constant__ CUtensorMap tmEo, const __grid_constant__ CUtensorMap tmH)
 {
-    using T = G4<FD, RPT4B>;
-    constexpr int K = T::K, SN = T::SN, SH = T::SH, RPT = RPT4B;
-    constexpr int STG = L4<FD>::ADB_STAGE, OWNB = 3 * T::TZH * TX4 * 4, PL = T::TZH * TX4;
+    using T = G4<FD, RPT>;
+    constexpr int K = T::K, SN = T::SN, SH = T::SH;
+    constexpr int STG = L4<FD, RPT>::ADB_STAGE, OWNB = 3 * T::TZH * TX4 * 4, PL = T::TZH * TX4;
     extern __shared__ __align__(128) float sm[];
     constexpr int NCC = (SW4 + TX - 1) / TX;
     float *aZXZ = sm + 2 * STG, *aXXZ = aZXZ + T::S1;
@@ -986,9 +986,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
     // coefficient tables: x sets (A, B of the transposed D+ of P, A, B of
     // the transposed D- of Q), z sets (A, B of the transposed D+ of Q, A, B
     // of the transposed D- of P)
-    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD>::ADB);
+    float4 *xt = reinterpret_cast<float4 *>(sm + L4<FD, RPT>::ADB);
     float4 *zt = xt + 4 * TX4;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD>::ADB);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + L5<FD, RPT>::ADB);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const Ctx3 c = ctx5(g, spg, T::TZH, tiles_x, g.tordB, g.theavyB);
     const int nsh = c.s1 - c.s0;
@@ -1006,7 +1006,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(sm + b * STG, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
             tma_load_4d(sm + b * STG + T::S2, &tmEo, bar + b, c.j0, c.i0, F_EX, c.s0 + b);
-            if (htma) tma_load_4d(sm + b * STG + T::S2 + L4<FD>::OWNB3, &tmH, bar + b, hx, hy, hz, c.s0 + b);
+            if (htma) tma_load_4d(sm + b * STG + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + b, hx, hy, hz, c.s0 + b);
         }
     }
     __syncthreads();
@@ -1072,7 +1072,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
         const int s = c.s0 + it;
         float *S = sm + (it & 1) * STG;
         const float *own = S + T::S2;   // [ex_a, ez_a, es_a][TZH][TX4] of the tile's own cells
-        const float *hown = own + L4<FD>::OWNB3;   // [sxx, szz, sxz][TZH][TX4] carry-in (htma)
+        const float *hown = own + L4<FD, RPT>::OWNB3;   // [sxx, szz, sxz][TZH][TX4] carry-in (htma)
         float *exa = A + ((long long)s * F_N + F_EX) * g.fstride;
         float *eza = A + ((long long)s * F_N + F_EZ) * g.fstride;
         float *esa = A + ((long long)s * F_N + F_ES) * g.fstride;
@@ -1399,7 +1399,7 @@ __global__ void __launch_bounds__(NTHR, STFWI_V4_MINBLOCKS)
             mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(S, &tmPQ, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
             tma_load_4d(S + T::S2, &tmEo, bar + (it & 1), c.j0, c.i0, F_EX, s + 2);
-            if (htma) tma_load_4d(S + T::S2 + L4<FD>::OWNB3, &tmH, bar + (it & 1), hx, hy, hz, s + 2);
+            if (htma) tma_load_4d(S + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + (it & 1), hx, hy, hz, s + 2);
         }
         if (n > 0) {
             const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];

@@ -60,9 +60,11 @@ struct stfwi_handle {
     CUtensorMap tmH{};        // history [shot][slot*snf + field][nz_dom][nx_dom] (own-cell carry-in boxes)
     bool hist_tma = false;    // tmH valid: pad and nx_dom multiples of 4 (16-byte box rows)
     // staged tilings: tiles tw columns wide; fwd_vel/fwd_str/adj_a tiles tha
-    // rows high, adj_b tiles thb rows high
-    int tw = TX4, tha = RPT4 * NWARP, thb = RPT4B * NWARP;
+    // = ra * NWARP rows high, adj_b tiles thb = rb * NWARP rows high (ra, rb:
+    // rows per thread, 1 or 2, set by set_tiling)
+    int tw = TX4, ra = RPT_DEFAULT, rb = RPT_DEFAULT, tha = RPT_DEFAULT * NWARP, thb = RPT_DEFAULT * NWARP;
     int ntx = 1, ntza = 1, ntzb = 1;                       // tile counts
+    int ntz_max = 1;                                       // tile rows of the lowest tiles (array sizes)
     int *tile_startA = nullptr, *tile_recA = nullptr;      // receivers grouped by the tw x tha tiles
     int *tile_startB = nullptr, *tile_recB = nullptr;      // receivers grouped by the tw x thb tiles
     int *tordA = nullptr, *tordB = nullptr;                // tile dispatch orders, boundary tiles first
@@ -421,45 +423,67 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
     else cudaEventRecord(h->pev[k][idx], st);
 }
 
-template <int FD>
-void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+template <int FD, int R>
+void launch_fwd_step_r(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
+    using Lk = L5<FD, R>;
     const int tiles = h->ntx * h->ntza;
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
     prof_mark(h, 0, n, 0, st);
-    st_fwd_vel<FD><<<dim3(tiles, h->grp[0]), block, L5<FD>::bytes(L5<FD>::VEL, 2), st>>>(
+    st_fwd_vel<FD, R><<<dim3(tiles, h->grp[0]), block, Lk::bytes(Lk::VEL, 2), st>>>(
         h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
-    auto str = o.energy ? st_fwd_str<FD, true> : st_fwd_str<FD, false>;
-    str<<<dim3(tiles, h->grp[1]), block, L5<FD>::bytes(L5<FD>::STR, 2), st>>>(
+    auto str = o.energy ? st_fwd_str<FD, R, true> : st_fwd_str<FD, R, false>;
+    str<<<dim3(tiles, h->grp[1]), block, Lk::bytes(Lk::STR, 2), st>>>(
         h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
     prof_mark(h, 1, n, 1, st);
 }
 
-
 template <int FD>
-void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
 {
-    dim3 block(TX, NWARP);
+    if (h->ra == 1) launch_fwd_step_r<FD, 1>(h, n, o, st);
+    else launch_fwd_step_r<FD, 2>(h, n, o, st);
+}
+
+template <int FD, int R>
+void launch_adj_a_r(stfwi_handle *h, int n, const AdjIn &ai, cudaStream_t st)
+{
+    using Lk = L5<FD, R>;
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
-    prof_mark(h, 2, n, 0, st);
-    st_adj_a<FD><<<dim3(h->ntx * h->ntza, h->grp[2]), block, L5<FD>::bytes(L5<FD>::ADA, 2), st>>>(
+    st_adj_a<FD, R><<<dim3(h->ntx * h->ntza, h->grp[2]), dim3(TX, NWARP), Lk::bytes(Lk::ADA, 2), st>>>(
         h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
-    prof_mark(h, 2, n, 1, st);
-    prof_mark(h, 3, n, 0, st);
+}
+
+template <int FD, int R>
+void launch_adj_b_r(stfwi_handle *h, int n, const AdjOut &ao, cudaStream_t st)
+{
+    using Lk = L5<FD, R>;
+    Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
     auto launch = [&](auto kern) {
-        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), block, L5<FD>::bytes(L5<FD>::ADB, 2), st>>>(
+        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), dim3(TX, NWARP), Lk::bytes(Lk::ADB, 2), st>>>(
             h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
             h->tmPQ, h->tmEo, h->tmH);
     };
     const bool rho = h->g.snf == 5;
-    if (ao.want_exact && ao.want_img) rho ? launch(st_adj_b<FD, true, true, true>) : launch(st_adj_b<FD, true, true, false>);
-    else if (ao.want_exact) rho ? launch(st_adj_b<FD, true, false, true>) : launch(st_adj_b<FD, true, false, false>);
-    else if (ao.want_img) rho ? launch(st_adj_b<FD, false, true, true>) : launch(st_adj_b<FD, false, true, false>);
-    else launch(st_adj_b<FD, false, false, false>);
+    if (ao.want_exact && ao.want_img) rho ? launch(st_adj_b<FD, R, true, true, true>) : launch(st_adj_b<FD, R, true, true, false>);
+    else if (ao.want_exact) rho ? launch(st_adj_b<FD, R, true, false, true>) : launch(st_adj_b<FD, R, true, false, false>);
+    else if (ao.want_img) rho ? launch(st_adj_b<FD, R, false, true, true>) : launch(st_adj_b<FD, R, false, true, false>);
+    else launch(st_adj_b<FD, R, false, false, false>);
+}
+
+template <int FD>
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+{
+    prof_mark(h, 2, n, 0, st);
+    if (h->ra == 1) launch_adj_a_r<FD, 1>(h, n, ai, st);
+    else launch_adj_a_r<FD, 2>(h, n, ai, st);
+    prof_mark(h, 2, n, 1, st);
+    prof_mark(h, 3, n, 0, st);
+    if (h->rb == 1) launch_adj_b_r<FD, 1>(h, n, ao, st);
+    else launch_adj_b_r<FD, 2>(h, n, ao, st);
     prof_mark(h, 3, n, 1, st);
 }
 
@@ -675,25 +699,32 @@ stfwi_status set_smem(stfwi_handle *h, const void *const (&kern)[7])
     return STFWI_OK;
 }
 
+template <int FD, int R>
+stfwi_status setup_tma_kernels_r(stfwi_handle *h)
+{
+    using Lk = L5<FD, R>;
+    const void *const kern[7] = {
+        (const void *)st_fwd_vel<FD, R>, (const void *)st_fwd_str<FD, R, false>, (const void *)st_adj_a<FD, R>,
+        (const void *)st_adj_b<FD, R, true, false, false>, (const void *)st_adj_b<FD, R, true, true, false>,
+        (const void *)st_adj_b<FD, R, false, true, false>, (const void *)st_adj_b<FD, R, false, false, false>};
+    stfwi_status r = set_smem<Lk>(h, kern);
+    if (r) return r;
+    CK(h, cudaFuncSetAttribute((const void *)st_fwd_str<FD, R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)Lk::bytes(Lk::STR, 2)));
+    const void *const rho_kern[3] = {(const void *)st_adj_b<FD, R, true, false, true>,
+                                     (const void *)st_adj_b<FD, R, true, true, true>,
+                                     (const void *)st_adj_b<FD, R, false, true, true>};
+    for (const void *k : rho_kern)
+        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lk::bytes(Lk::ADB, 2)));
+    return STFWI_OK;
+}
+
+// both tile heights of every kernel of the fd order
 template <int FD>
 stfwi_status setup_tma_kernels(stfwi_handle *h)
 {
-    const void *const kern[7] = {
-        (const void *)st_fwd_vel<FD>, (const void *)st_fwd_str<FD, false>, (const void *)st_adj_a<FD>,
-        (const void *)st_adj_b<FD, true, false, false>, (const void *)st_adj_b<FD, true, true, false>,
-        (const void *)st_adj_b<FD, false, true, false>, (const void *)st_adj_b<FD, false, false, false>};
-    stfwi_status r = set_smem<L5<FD>>(h, kern);
-    if (r) return r;
-    CK(h, cudaFuncSetAttribute((const void *)st_fwd_str<FD, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)L5<FD>::bytes(L5<FD>::STR, 2)));
-    const void *const rho_kern[3] = {(const void *)st_adj_b<FD, true, false, true>,
-                                     (const void *)st_adj_b<FD, true, true, true>,
-                                     (const void *)st_adj_b<FD, false, true, true>};
-    for (const void *k : rho_kern)
-        CK(h, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)L5<FD>::bytes(L5<FD>::ADB, 2)));
-    return STFWI_OK;
-
+    stfwi_status r = setup_tma_kernels_r<FD, 1>(h);
+    return r ? r : setup_tma_kernels_r<FD, 2>(h);
 }
 
 stfwi_status setup_tensor_maps(stfwi_handle *h)
@@ -772,6 +803,56 @@ std::vector<int> tile_order(const Geo &g, int K, int tw, int th, int ntx, int nt
     *heavy = (int)hv.size();
     hv.insert(hv.end(), lt.begin(), lt.end());
     return hv;
+}
+
+// receivers grouped by the tiles of the two staged tilings (CSR: start per
+// tile, receiver indices)
+static stfwi_status group_receivers(stfwi_handle *h)
+{
+    const Geo &g = h->g;
+    const int nrec = (int)h->rec_x_h.size();
+    auto tile_of = [&](int r, int th) { return ((h->rec_z_h[r] + g.z0) / th) * h->ntx + (h->rec_x_h[r] + g.pad) / h->tw; };
+    auto group = [&](int th, int ntz, int *d_start, int *d_list) -> stfwi_status {
+        const int ntl = h->ntx * ntz;
+        std::vector<int> c(ntl + 1, 0), st(ntl + 1, 0), l(std::max(nrec, 1));
+        for (int r = 0; r < nrec; ++r) c[tile_of(r, th)]++;
+        for (int t = 0; t < ntl; ++t) st[t + 1] = st[t] + c[t];
+        std::vector<int> f(st.begin(), st.end() - 1);
+        for (int r = 0; r < nrec; ++r) l[f[tile_of(r, th)]++] = r;
+        CK(h, cudaMemcpy(d_start, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
+        CK(h, cudaMemcpy(d_list, l.data(), l.size() * 4, cudaMemcpyHostToDevice));
+        return STFWI_OK;
+    };
+    stfwi_status r = group(h->tha, h->ntza, h->tile_startA, h->tile_recA);
+    return r ? r : group(h->thb, h->ntzb, h->tile_startB, h->tile_recB);
+}
+
+// tile heights of the staged tilings: ra rows per thread (ra * NWARP rows a
+// tile) for fwd_vel, fwd_str and adj_a, rb for adj_b, each 1 or 2; sets the
+// tile counts, the dispatch orders, the receivers' tile lists and the tensor
+// maps whose boxes follow the heights, and drops the captured graphs
+static stfwi_status set_tiling(stfwi_handle *h, int ra, int rb)
+{
+    if ((ra != 1 && ra != 2) || (rb != 1 && rb != 2))
+        return fail(h, STFWI_ERR_INVALID, "rows per thread (%d, %d): use 1 or 2", ra, rb);
+    if (h->hs) CK(h, cudaStreamSynchronize(h->hs));   // no launch of the handle reads the old tables
+    Geo &g = h->g;
+    h->ra = ra; h->rb = rb;
+    h->tha = ra * NWARP; h->thb = rb * NWARP;
+    h->ntza = (g.nz + h->tha - 1) / h->tha;
+    h->ntzb = (g.nz + h->thb - 1) / h->thb;
+    const int K = h->d.fd_order / 2;
+    int ha = 0, hb = 0;
+    const std::vector<int> oa = tile_order(g, K, h->tw, h->tha, h->ntx, h->ntza, &ha);
+    const std::vector<int> ob = tile_order(g, K, h->tw, h->thb, h->ntx, h->ntzb, &hb);
+    CK(h, cudaMemcpy(h->tordA, oa.data(), oa.size() * 4, cudaMemcpyHostToDevice));
+    CK(h, cudaMemcpy(h->tordB, ob.data(), ob.size() * 4, cudaMemcpyHostToDevice));
+    g.tordA = h->tordA; g.tordB = h->tordB; g.theavyA = ha; g.theavyB = hb;
+    stfwi_status r = setup_tensor_maps(h);
+    if (r) return r;
+    if (h->recv_set && (r = group_receivers(h))) return r;
+    drop_graphs(h);
+    return STFWI_OK;
 }
 
 // ================================================================ C ABI
@@ -1004,10 +1085,9 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     g.snf = d->want_gradient == 2 ? 5 : 3;
     g.wait_polls = WAIT3;
     h->accp = g.snf == 5 ? 7 : 5;
-    h->tw = TX4; h->tha = RPT4 * NWARP; h->thb = RPT4B * NWARP;
+    h->tw = TX4;
     h->ntx = (int)((p.nx + h->tw - 1) / h->tw);
-    h->ntza = (int)((p.nz + h->tha - 1) / h->tha);
-    h->ntzb = (int)((p.nz + h->thb - 1) / h->thb);
+    h->ntz_max = (int)((p.nz + RPT_MIN * NWARP - 1) / (RPT_MIN * NWARP));
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
     {
         stfwi_status r = STFWI_OK;
@@ -1040,12 +1120,12 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
     ok &= alloc((void **)&h->sx, S * 4) && alloc((void **)&h->sz, S * 4) && alloc((void **)&h->stype, S * 4);
     ok &= alloc((void **)&h->wav, S * d->nt * 4) && alloc((void **)&h->fcoef, S * 4) &&
           alloc((void **)&h->mcoef, S * 4) && alloc((void **)&h->lm, S * 4);
-    ok &= alloc((void **)&h->tile_startA, ((size_t)h->ntx * h->ntza + 1) * 4) &&
-          alloc((void **)&h->tile_recA, nrec * 4) &&
-          alloc((void **)&h->tile_startB, ((size_t)h->ntx * h->ntzb + 1) * 4) &&
-          alloc((void **)&h->tile_recB, nrec * 4);
+    // tile arrays sized for the lowest tiles (set_tiling picks the heights)
+    const size_t ntl_max = (size_t)h->ntx * h->ntz_max;
+    ok &= alloc((void **)&h->tile_startA, (ntl_max + 1) * 4) && alloc((void **)&h->tile_recA, nrec * 4) &&
+          alloc((void **)&h->tile_startB, (ntl_max + 1) * 4) && alloc((void **)&h->tile_recB, nrec * 4);
     ok &= alloc((void **)&h->rx, nrec * 4) && alloc((void **)&h->rz, nrec * 4);
-    ok &= alloc((void **)&h->tordA, (size_t)h->ntx * h->ntza * 4) && alloc((void **)&h->tordB, (size_t)h->ntx * h->ntzb * 4);
+    ok &= alloc((void **)&h->tordA, ntl_max * 4) && alloc((void **)&h->tordB, ntl_max * 4);
     ok &= alloc((void **)&h->F, (size_t)S * F_N * NP * 4) && alloc((void **)&h->A, (size_t)S * F_N * NP * 4);
     ok &= alloc((void **)&h->PX, (size_t)S * NPX * p.nz * p.xs_n * 4) &&
           alloc((void **)&h->PZ, (size_t)S * NPZ * p.zs_n * p.P * 4);
@@ -1079,24 +1159,12 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_CUDA;
     }
     cudaMemset(h->status, 0, 16);
-    {
-        const int K = d->fd_order / 2;
-        int ha = 0, hb = 0;
-        const std::vector<int> oa = tile_order(g, K, h->tw, h->tha, h->ntx, h->ntza, &ha);
-        const std::vector<int> ob = tile_order(g, K, h->tw, h->thb, h->ntx, h->ntzb, &hb);
-        if (cudaMemcpy(h->tordA, oa.data(), oa.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-            cudaMemcpy(h->tordB, ob.data(), ob.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
-            stfwi_destroy(h);
-            return STFWI_ERR_CUDA;
-        }
-        g.tordA = h->tordA; g.tordB = h->tordB; g.theavyA = ha; g.theavyB = hb;
-    }
     // pitch padding and never-written cells read as zero by the tile copies
     cudaMemset(h->MATS, 0, (size_t)4 * NP * 4);
     cudaMemset(h->F, 0, (size_t)S * F_N * NP * 4);
     cudaMemset(h->A, 0, (size_t)S * F_N * NP * 4);
     {
-        stfwi_status r = setup_tensor_maps(h);
+        stfwi_status r = set_tiling(h, RPT_DEFAULT, RPT_DEFAULT);
         if (r) {
             fprintf(stderr, "stfwi_create: %s\n", h->err.c_str());
             stfwi_destroy(h);
@@ -1173,23 +1241,11 @@ stfwi_status stfwi_set_receivers(stfwi_handle *h, int32_t nrec, const int32_t *r
     }
     CK(h, cudaMemcpy(h->rx, rx.data(), rx.size() * 4, cudaMemcpyHostToDevice));
     CK(h, cudaMemcpy(h->rz, rz.data(), rz.size() * 4, cudaMemcpyHostToDevice));
-    // receivers grouped by the tiles of the two staged tilings
-    auto group = [&](int th, int ntz, int *d_start, int *d_list) -> stfwi_status {
-        const int ntl = h->ntx * ntz;
-        std::vector<int> c(ntl + 1, 0), st(ntl + 1, 0), l(std::max(nrec, 1));
-        for (int r = 0; r < nrec; ++r) c[(rz[r] / th) * h->ntx + rx[r] / h->tw]++;
-        for (int t = 0; t < ntl; ++t) st[t + 1] = st[t] + c[t];
-        std::vector<int> f(st.begin(), st.end() - 1);
-        for (int r = 0; r < nrec; ++r) l[f[(rz[r] / th) * h->ntx + rx[r] / h->tw]++] = r;
-        CK(h, cudaMemcpy(d_start, st.data(), st.size() * 4, cudaMemcpyHostToDevice));
-        CK(h, cudaMemcpy(d_list, l.data(), l.size() * 4, cudaMemcpyHostToDevice));
-        return STFWI_OK;
-    };
-    stfwi_status gr;
-    if ((gr = group(h->tha, h->ntza, h->tile_startA, h->tile_recA))) return gr;
-    if ((gr = group(h->thb, h->ntzb, h->tile_startB, h->tile_recB))) return gr;
     h->rec_x_h.assign(rec_x, rec_x + nrec);
     h->rec_z_h.assign(rec_z, rec_z + nrec);
+    h->recv_set = false;
+    stfwi_status gr = group_receivers(h);
+    if (gr) return gr;
     h->recv_set = true;
     return STFWI_OK;
 }
@@ -1616,11 +1672,20 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
         for (auto &e : h->pev[k]) CK(h, cudaEventCreate(&e));
     }
     h->prof_every = 1;
-    static const int cand[] = {1, 2, 3, 4, 5, 6, 8};
-    double best[4] = {1e300, 1e300, 1e300, 1e300};
-    int pick[4] = {h->spgk[0], h->spgk[1], h->spgk[2], h->spgk[3]};
+    // shots per block up to 25: with boundary tiles dispatched first, large
+    // groups (fewer, longer blocks per tile) can pay on grids with many
+    // boundary tiles; and both tile heights (rows per thread 1, 2: 8- and
+    // 16-row tiles)
+    static const int cand[] = {1, 2, 3, 4, 5, 6, 8, 10, 13, 17, 25};
+    double best[2][4];
+    int pick[2][4];
+    for (int q = 0; q < 2; ++q)
+        for (int k = 0; k < 4; ++k) { best[q][k] = 1e300; pick[q][k] = h->spgk[k]; }
+    const int ra0 = h->ra, rb0 = h->rb;
     stfwi_status r = STFWI_OK;
-    for (int c : cand) {
+    for (int q = 0; q < 2 && !r; ++q) {
+      if ((r = set_tiling(h, q + 1, q + 1))) break;
+      for (int c : cand) {
         if (c > h->nshot) break;
         const int spg[4] = {c, c, c, c};
         set_groups(h, spg);
@@ -1646,7 +1711,8 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
-            r = fail(h, STFWI_ERR_CUDA, "autotune pass with %d shots per block: %s", c, cudaGetErrorString(e));
+            r = fail(h, STFWI_ERR_CUDA, "autotune pass with %d shots per block, %d-row tiles: %s", c, 8 * (q + 1),
+                     cudaGetErrorString(e));
             break;
         }
         for (int k = 0; k < 4; ++k) {
@@ -1655,8 +1721,9 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
                 float e = 0.f;
                 if (cudaEventElapsedTime(&e, h->pev[k][2 * n], h->pev[k][2 * n + 1]) == cudaSuccess) ms += e;
             }
-            if (ms < best[k]) { best[k] = ms; pick[k] = c; }
+            if (ms < best[q][k]) { best[q][k] = ms; pick[q][k] = c; }
         }
+      }
     }
     cudaGetLastError();
     for (int k = 0; k < 4; ++k) {
@@ -1664,13 +1731,39 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
         h->pev[k].swap(saved[k]);
     }
     h->prof_every = saved_every;
-    if (r) return r;
-    for (int k = 0; k < 4; ++k) h->tuned[k] = pick[k];
-    set_groups(h, pick);
+    if (r) {
+        set_tiling(h, ra0, rb0);
+        return r;
+    }
+    // fwd_vel, fwd_str and adj_a share a tiling (the receivers' tile lists):
+    // the height with the lower sum of their best times; adj_b its own
+    const double sa[2] = {best[0][0] + best[0][1] + best[0][2], best[1][0] + best[1][1] + best[1][2]};
+    const int qa = sa[0] < sa[1] ? 0 : 1, qb = best[0][3] < best[1][3] ? 0 : 1;
+    if ((r = set_tiling(h, qa + 1, qb + 1))) return r;
+    const int spg[4] = {pick[qa][0], pick[qa][1], pick[qa][2], pick[qb][3]};
+    for (int k = 0; k < 4; ++k) h->tuned[k] = spg[k];
+    set_groups(h, spg);
     drop_graphs(h);
     h->stored = false;   // the timing passes overwrote the state
     if (spg_out)
-        for (int k = 0; k < 4; ++k) spg_out[k] = pick[k];
+        for (int k = 0; k < 4; ++k) spg_out[k] = spg[k];
+    return STFWI_OK;
+}
+
+stfwi_status stfwi_set_tile_rows(stfwi_handle *h, int32_t rows_a, int32_t rows_b)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    if (rows_a % NWARP || rows_b % NWARP)
+        return fail(h, STFWI_ERR_INVALID, "tile rows (%d, %d): use 8 or 16", rows_a, rows_b);
+    // the state and a kept history do not depend on the tiling
+    return set_tiling(h, rows_a / NWARP, rows_b / NWARP);
+}
+
+stfwi_status stfwi_tile_rows(const stfwi_handle *h, int32_t *rows_out)
+{
+    if (!h || !rows_out) return STFWI_ERR_INVALID;
+    rows_out[0] = h->tha;
+    rows_out[1] = h->thb;
     return STFWI_OK;
 }
 

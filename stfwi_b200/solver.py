@@ -294,12 +294,23 @@ class Solver:
         return {k: (float(out[2 * i]), int(out[2 * i + 1])) for i, k in enumerate(self.KERNELS)}
 
     def autotune(self, steps=20):
-        """Pick the shots per block of each stencil kernel by timing `steps`
-        forward and adjoint steps per candidate; returns {kernel: shots per
-        block}.  Overwrites the state: call before the forward of a gradient."""
+        """Pick the tile shapes and the shots per block of each stencil kernel
+        by timing `steps` forward and adjoint steps per candidate; returns
+        {kernel: shots per block} (``tile_rows()`` gives the shapes).
+        Overwrites the state: call before the forward of a gradient."""
         out = np.zeros(4, dtype=np.int32)
         self._ok(self.lib.stfwi_autotune(self.h, int(steps), out.ctypes.data, _stream()), "autotune")
         return dict(zip(self.KERNELS, (int(v) for v in out)))
+
+    def tile_rows(self):
+        """(rows of the fwd_vel/fwd_str/adj_a tiles, rows of the adj_b tiles); tiles are 64 columns wide."""
+        out = np.zeros(2, dtype=np.int32)
+        self._ok(self.lib.stfwi_tile_rows(self.h, out.ctypes.data), "tile_rows")
+        return int(out[0]), int(out[1])
+
+    def set_tile_rows(self, rows_a, rows_b):
+        """Tile heights (8 or 16 rows) of fwd_vel/fwd_str/adj_a and of adj_b."""
+        self._ok(self.lib.stfwi_set_tile_rows(self.h, int(rows_a), int(rows_b)), "set_tile_rows")
 
     def set_postprocess(self, grad_smooth_sigma=None, source_taper=None, illumination=None):
         """Post-processing applied on the device to the gradients that

@@ -31,8 +31,9 @@ def _solver(nt, nrec, nshot, fd, fs, want_gradient=False, pad=C.PAD, nz=C.NZ, nx
 
 
 
+@pytest.mark.parametrize("tiles", [(16, 16), (8, 8)])
 @pytest.mark.parametrize("fd,fs,st", C.CONFIGS)
-def test_forward_and_adjoint_vs_oracle(fd, fs, st):
+def test_forward_and_adjoint_vs_oracle(fd, fs, st, tiles):
     """The reference's dot-product case (test_adjoint_kernel.py) on the GPU:
     seismograms and the source adjoint against the FP64 oracle, and the
     dot-product identity of the FP32 kernels."""
@@ -40,6 +41,7 @@ def test_forward_and_adjoint_vs_oracle(fd, fs, st):
     sx, sz, rx, rz = C.acquisition(fs, st)
     s_in, ys = C.random_vectors()
     S = _solver(C.NT, len(rx), 1, fd, fs)
+    S.set_tile_rows(*tiles)
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots([sx], [sz], [st], s_in.astype(np.float32))
@@ -211,8 +213,9 @@ def _smooth_model(nz, nx, seed):
     return vs, vp, rho
 
 
+@pytest.mark.parametrize("tiles", [(16, 16), (8, 8), (16, 8), (8, 16)])
 @pytest.mark.parametrize("fd,fs", [(8, True), (8, False), (4, True), (2, False)])
-def test_multi_tile_grid_vs_oracle(fd, fs):
+def test_multi_tile_grid_vs_oracle(fd, fs, tiles):
     """A grid of several tiles in x and z (interior tiles without the C-PML
     fix-up, tile edges inside the stencil reach), with sources and receivers
     near tile edges: seismograms, misfit and the exact gradient against the
@@ -223,7 +226,7 @@ def test_multi_tile_grid_vs_oracle(fd, fs):
     vs, vp, rho = _smooth_model(nz, nx, 7)
     rx = np.arange(0, nx, 3, dtype=np.int32)
     rz = np.full_like(rx, 0 if fs else 3)
-    rz[::4] = 31                      # a tile-row edge in z (tiles of 16 and 32 rows)
+    rz[::4] = 31                      # a tile-row edge in z (tiles of 8 and 16 rows)
     # 44 + pad = 54: two columns below a 64-column tile edge; the second and
     # third sources sit inside interior tiles (rows 16-31 and 32-47, columns 64-127)
     sx = np.array([44, 54, 70])
@@ -239,6 +242,8 @@ def test_multi_tile_grid_vs_oracle(fd, fs):
     (gx_vs, gx_vp, _), loss = O.compute_gradient("ad", Vs=vs, Vp=vp, rho=rho, **kw)
     S = _solver(nt, len(rx), 3, fd, fs, want_gradient=True, pad=pad, nz=nz, nx=nx, dx=dx, dz=dz, dt=dt,
                 fc=fc)
+    S.set_tile_rows(*tiles)
+    assert S.tile_rows() == tiles
     S.set_model(vs, vp, rho)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav.astype(np.float32))
@@ -252,7 +257,7 @@ def test_multi_tile_grid_vs_oracle(fd, fs):
     g = S.gradient(exact=True)
     errs = {"misfit": abs(mis.sum() / loss - 1), "exact_vs": _rel(g["exact"][0], gx_vs),
             "exact_vp": _rel(g["exact"][1], gx_vp)}
-    print(f"multi-tile fd{fd} fs={fs}: amplification {amp:.1f} errors {errs}")
+    print(f"multi-tile fd{fd} fs={fs} tiles {tiles}: amplification {amp:.1f} errors {errs}")
     tol = 2e-5 * max(amp, 1.0)
     assert all(e < tol for e in errs.values()), (tol, errs)
     S.close()
@@ -339,10 +344,25 @@ def test_density_gradient_checkpointed_equals_store_all():
         assert _rel(a, b) < 1e-12, _rel(a, b)
 
 
+def test_tile_rows_are_checked():
+    """Tile heights of 8 and 16 rows are accepted; other values are refused
+    (ValueError) and leave the tiling unchanged."""
+    S = _solver(10, 4, 1, 8, True)
+    assert S.tile_rows() == (16, 16)
+    for bad in ((12, 16), (16, 0), (24, 8), (32, 32), (-8, 16)):
+        with pytest.raises(ValueError):
+            S.set_tile_rows(*bad)
+    assert S.tile_rows() == (16, 16)
+    S.set_tile_rows(8, 16)
+    assert S.tile_rows() == (8, 16)
+    S.close()
+
+
 def test_autotuned_schedule_gives_the_same_gradient():
-    """stfwi_autotune picks shots per block for each kernel by timing; the
-    gradient computed with the tuned schedule equals the default schedule's
-    (the grouping only changes the summation order of a launch's shots)."""
+    """stfwi_autotune picks the tile shapes and the shots per block of each
+    kernel by timing; the gradient computed with the tuned schedule equals
+    the default schedule's (the grouping only changes the summation order of
+    a launch's shots)."""
     vs, vp, rho = C.model()
     nt, fd, fs = 90, 8, True
     rx = np.arange(1, C.NX - 1, 3, dtype=np.int32)
@@ -361,7 +381,8 @@ def test_autotuned_schedule_gives_the_same_gradient():
         if tune:
             pick = S.autotune(steps=10)
             assert set(pick) == {"fwd_vel", "fwd_str", "adj_a", "adj_b"}
-            assert all(v in (1, 2, 3, 4, 5, 6, 8) for v in pick.values()), pick
+            assert all(v in (1, 2, 3, 4, 5, 6, 8, 10, 13, 17, 25) for v in pick.values()), pick
+            assert all(r in (8, 16) for r in S.tile_rows()), S.tile_rows()
         S.forward(store=True)
         mis = S.misfit(obs, 1, 1.0)
         g = S.gradient(exact=True, imaging=True)
