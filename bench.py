@@ -194,7 +194,9 @@ def run_reference(args, rank, world):
         return
     cfg = workload(args.nt, args.shots)
     ncores = os.cpu_count() or 1
-    nshot, nt = cpu_sample(cfg, ncores)
+    # 200 steps a sample (about 5 s on 16 cores), so that warm-up plus timed
+    # samples stay within a few minutes
+    nshot, nt = cpu_sample(cfg, ncores, nt=200)
     from oracle import oracle as O
     O.lib_fast()
     vals = []
