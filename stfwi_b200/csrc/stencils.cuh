@@ -1006,7 +1006,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
             mbar_arrive_expect_tx(bar + b, 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(sm + b * STG, &tmPQ, bar + b, c.j0 - XO4, c.i0 - K, F_U, c.s0 + b);
             tma_load_4d(sm + b * STG + T::S2, &tmEo, bar + b, c.j0, c.i0, F_EX, c.s0 + b);
-            if (htma) tma_load_4d(sm + b * STG + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + b, hx, hy, hz, c.s0 + b);
+            if (htma)
+                tma_load_4d_hint(sm + b * STG + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + b, hx, hy, hz, c.s0 + b,
+                                 l2_evict_first());
         }
     }
     __syncthreads();
@@ -1399,7 +1401,9 @@ __global__ void __launch_bounds__(NTHR, STFWI_MINBLOCKS)
             mbar_arrive_expect_tx(bar + (it & 1), 2 * SN * 4 + OWNB + hbytes);
             tma_load_4d(S, &tmPQ, bar + (it & 1), c.j0 - XO4, c.i0 - K, F_U, s + 2);
             tma_load_4d(S + T::S2, &tmEo, bar + (it & 1), c.j0, c.i0, F_EX, s + 2);
-            if (htma) tma_load_4d(S + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + (it & 1), hx, hy, hz, s + 2);
+            if (htma)
+                tma_load_4d_hint(S + T::S2 + L4<FD, RPT>::OWNB3, &tmH, bar + (it & 1), hx, hy, hz, s + 2,
+                                 l2_evict_first());
         }
         if (n > 0) {
             const int r0 = rv.tile_start[c.tile], r1 = rv.tile_start[c.tile + 1];
