@@ -358,10 +358,24 @@ def evaluate_multiband(net, seeds, K=4, bands=BANDS, iters=20, geom=I.GEOMETRY, 
 
 
 def summarize(records):
+    """Ratios of the models whose learned run reached the target
+    (``median_time_ratio``), and the stricter median over the models on
+    which the plain method improved on its start at all, a model the learned
+    run did not bring to the target counting as an infinite ratio
+    (``median_time_ratio_counting_misses``; None when that median is a miss).
+    A model whose plain run never improved on the start has its start error
+    as the target, which any run "reaches" at time zero: such models are
+    counted in ``plain_no_progress`` and left out of the strict median."""
     ratios = [r["ratio"] for r in records if r["ratio"] is not None]
     after = [r["err_after_learned_step"] for r in records if r["err_after_learned_step"] is not None]
+    progress = [r for r in records if r["target"] < r["err_start"]]
+    strict = [r["ratio"] if r["ratio"] is not None else np.inf for r in progress]
+    med_strict = float(np.median(strict)) if strict else None
     return dict(models=len(records), reached_target=sum(r["learned_time_s"] is not None for r in records),
                 learned_step_accepted=sum(bool(r["learned_step_accepted"]) for r in records),
+                plain_no_progress=len(records) - len(progress),
+                median_time_ratio_counting_misses=med_strict if med_strict is not None and np.isfinite(med_strict)
+                else None,
                 median_time_ratio=float(np.median(ratios)) if ratios else None,
                 mean_time_ratio=float(np.mean(ratios)) if ratios else None,
                 median_err_start=float(np.median([r["err_start"] for r in records])),

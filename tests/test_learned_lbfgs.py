@@ -118,6 +118,17 @@ def test_experiment_features_and_summary():
     s = E.summarize(recs)
     assert s["models"] == 3 and s["reached_target"] == 2 and s["learned_step_accepted"] == 2
     assert abs(s["median_time_ratio"] - 0.4) < 1e-12 and abs(s["median_err_after_learned_step"] - 0.05075) < 1e-12
+    # the miss counts as an infinite ratio: median of (0.2, inf, 0.6) is 0.6
+    assert s["plain_no_progress"] == 0 and abs(s["median_time_ratio_counting_misses"] - 0.6) < 1e-12
+    # a model on which the plain run never improved on its start (target =
+    # start error, "reached" at once) stays out of the strict median
+    recs.append(dict(ratio=0.0, learned_time_s=0.0, learned_step_accepted=False, err_start=0.06, target=0.06,
+                     err_after_learned_step=None))
+    s = E.summarize(recs)
+    assert s["plain_no_progress"] == 1 and abs(s["median_time_ratio_counting_misses"] - 0.6) < 1e-12
+    recs.append(dict(ratio=None, learned_time_s=None, learned_step_accepted=True, err_start=0.07, target=0.06,
+                     err_after_learned_step=0.065))
+    assert E.summarize(recs)["median_time_ratio_counting_misses"] is None   # the median is a miss
 
 
 def test_acquisition_and_model_pair():
