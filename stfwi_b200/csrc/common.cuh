@@ -58,6 +58,7 @@ struct Geo {
     // or the free surface first, or null for the plain order
     const int *tordA, *tordB;
     int theavyA, theavyB;
+    int goff;                  // first shot group of the launch (a pass split into two chains)
 };
 
 struct Mat {

@@ -222,7 +222,7 @@ __device__ __forceinline__ Ctx3 ctx5(const Geo &g, int spg, int tzh, int tiles_x
     c.tile = t;
     c.j0 = (t % tiles_x) * TX4;
     c.i0 = (t / tiles_x) * tzh;
-    c.s0 = grp * spg;
+    c.s0 = (grp + g.goff) * spg;
     c.s1 = min(c.s0 + spg, g.nshot);
     return c;
 }

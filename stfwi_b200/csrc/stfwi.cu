@@ -110,7 +110,8 @@ struct stfwi_handle {
     bool stored = false;  // last forward kept its strain history
 
     cudaStream_t hs = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    cudaStream_t hs2 = nullptr;   // second chain of a pass split over the shot groups
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr;
     // sampled kernel timing: pev[k] holds (start, stop) pairs per sampled step
     int prof_every = 0;
     std::vector<cudaEvent_t> pev[4];
@@ -423,48 +424,78 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
     else cudaEventRecord(h->pev[k][idx], st);
 }
 
+// the shot groups of kernel k that a launch covers: all of them (part < 0),
+// the first half (part 0) or the rest (part 1) -- the two chains of a split
+// pass; the Geo of the launch carries the first group
+Geo part_geo(const stfwi_handle *h, int k, int part, int *ngroups)
+{
+    Geo g = h->g;
+    const int G = h->grp[k], GA = (G + 1) / 2;
+    g.goff = part == 1 ? GA : 0;
+    *ngroups = part < 0 ? G : part == 0 ? GA : G - GA;
+    return g;
+}
+
+// a pass may run as two independent chains over the shot groups (the shots
+// never interact, the shared sums are atomic) when every stencil kernel
+// groups the shots the same way -- a chain's kernels then touch exactly its
+// own shots -- there are at least two groups, and no sampled timing is on
+bool two_chains(const stfwi_handle *h)
+{
+    for (int k = 1; k < 4; ++k)
+        if (h->spgk[k] != h->spgk[0] || h->grp[k] != h->grp[0]) return false;
+    return h->grp[0] >= 2 && h->prof_every == 0 && h->hs2 != nullptr;
+}
+
 template <int FD, int R>
-void launch_fwd_step_r(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void launch_fwd_step_r(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st, int part)
 {
     using Lk = L5<FD, R>;
     const int tiles = h->ntx * h->ntza;
     dim3 block(TX, NWARP);
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
+    int ng = 0;
+    const Geo g0 = part_geo(h, 0, part, &ng);
     prof_mark(h, 0, n, 0, st);
-    st_fwd_vel<FD, R><<<dim3(tiles, h->grp[0]), block, Lk::bytes(Lk::VEL, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
+    st_fwd_vel<FD, R><<<dim3(tiles, ng), block, Lk::bytes(Lk::VEL, 2), st>>>(
+        g0, mat_of(h), shots_of(h), h->F, h->PX, h->PZ, n, h->spgk[0], h->ntx, h->status, h->tmS, h->tmUo);
     prof_mark(h, 0, n, 1, st);
     prof_mark(h, 1, n, 0, st);
+    const Geo g1 = part_geo(h, 1, part, &ng);
     auto str = o.energy ? st_fwd_str<FD, R, true> : st_fwd_str<FD, R, false>;
-    str<<<dim3(tiles, h->grp[1]), block, Lk::bytes(Lk::STR, 2), st>>>(
-        h->g, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
+    str<<<dim3(tiles, ng), block, Lk::bytes(Lk::STR, 2), st>>>(
+        g1, mat_of(h), shots_of(h), rva, h->F, h->PX, h->PZ, n, h->spgk[1], h->ntx, o, h->tmV, h->tmSo);
     prof_mark(h, 1, n, 1, st);
 }
 
 template <int FD>
-void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void launch_fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st, int part)
 {
-    if (h->ra == 1) launch_fwd_step_r<FD, 1>(h, n, o, st);
-    else launch_fwd_step_r<FD, 2>(h, n, o, st);
+    if (h->ra == 1) launch_fwd_step_r<FD, 1>(h, n, o, st, part);
+    else launch_fwd_step_r<FD, 2>(h, n, o, st, part);
 }
 
 template <int FD, int R>
-void launch_adj_a_r(stfwi_handle *h, int n, const AdjIn &ai, cudaStream_t st)
+void launch_adj_a_r(stfwi_handle *h, int n, const AdjIn &ai, cudaStream_t st, int part)
 {
     using Lk = L5<FD, R>;
     Recv rva{h->tile_startA, h->tile_recA, h->rx, h->rz};
-    st_adj_a<FD, R><<<dim3(h->ntx * h->ntza, h->grp[2]), dim3(TX, NWARP), Lk::bytes(Lk::ADA, 2), st>>>(
-        h->g, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
+    int ng = 0;
+    const Geo ga = part_geo(h, 2, part, &ng);
+    st_adj_a<FD, R><<<dim3(h->ntx * h->ntza, ng), dim3(TX, NWARP), Lk::bytes(Lk::ADA, 2), st>>>(
+        ga, mat_of(h), rva, h->A, h->PX, h->PZ, n, h->spgk[2], h->ntx, ai, h->status, h->tmE, h->tmPQo);
 }
 
 template <int FD, int R>
-void launch_adj_b_r(stfwi_handle *h, int n, const AdjOut &ao, cudaStream_t st)
+void launch_adj_b_r(stfwi_handle *h, int n, const AdjOut &ao, cudaStream_t st, int part)
 {
     using Lk = L5<FD, R>;
     Recv rvb{h->tile_startB, h->tile_recB, h->rx, h->rz};
+    int ng = 0;
+    const Geo gb = part_geo(h, 3, part, &ng);
     auto launch = [&](auto kern) {
-        kern<<<dim3(h->ntx * h->ntzb, h->grp[3]), dim3(TX, NWARP), Lk::bytes(Lk::ADB, 2), st>>>(
-            h->g, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
+        kern<<<dim3(h->ntx * h->ntzb, ng), dim3(TX, NWARP), Lk::bytes(Lk::ADB, 2), st>>>(
+            gb, mat_of(h), shots_of(h), rvb, h->A, h->PX, h->PZ, n, h->spgk[3], h->ntx, ao, h->status,
             h->tmPQ, h->tmEo, h->tmH);
     };
     const bool rho = h->g.snf == 5;
@@ -475,15 +506,15 @@ void launch_adj_b_r(stfwi_handle *h, int n, const AdjOut &ao, cudaStream_t st)
 }
 
 template <int FD>
-void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st)
+void launch_adj_step(stfwi_handle *h, int n, const AdjIn &ai, const AdjOut &ao, cudaStream_t st, int part = -1)
 {
     prof_mark(h, 2, n, 0, st);
-    if (h->ra == 1) launch_adj_a_r<FD, 1>(h, n, ai, st);
-    else launch_adj_a_r<FD, 2>(h, n, ai, st);
+    if (h->ra == 1) launch_adj_a_r<FD, 1>(h, n, ai, st, part);
+    else launch_adj_a_r<FD, 2>(h, n, ai, st, part);
     prof_mark(h, 2, n, 1, st);
     prof_mark(h, 3, n, 0, st);
-    if (h->rb == 1) launch_adj_b_r<FD, 1>(h, n, ao, st);
-    else launch_adj_b_r<FD, 2>(h, n, ao, st);
+    if (h->rb == 1) launch_adj_b_r<FD, 1>(h, n, ao, st, part);
+    else launch_adj_b_r<FD, 2>(h, n, ao, st, part);
     prof_mark(h, 3, n, 1, st);
 }
 
@@ -564,13 +595,28 @@ stfwi_status copy_ckpt(stfwi_handle *h, int c, bool save, cudaStream_t st)
     return STFWI_OK;
 }
 
-void fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st)
+void fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st, int part = -1)
 {
     switch (h->d.fd_order) {
-    case 2: launch_fwd_step<2>(h, n, o, st); break;
-    case 4: launch_fwd_step<4>(h, n, o, st); break;
-    default: launch_fwd_step<8>(h, n, o, st); break;
+    case 2: launch_fwd_step<2>(h, n, o, st, part); break;
+    case 4: launch_fwd_step<4>(h, n, o, st, part); break;
+    default: launch_fwd_step<8>(h, n, o, st, part); break;
     }
+}
+
+// fork the handle's second stream off `st` / join it back (event edges of
+// the captured graph)
+stfwi_status fork_chain(stfwi_handle *h, cudaStream_t st)
+{
+    CK(h, cudaEventRecord(h->ev_fork, st));
+    CK(h, cudaStreamWaitEvent(h->hs2, h->ev_fork, 0));
+    return STFWI_OK;
+}
+stfwi_status join_chain(stfwi_handle *h, cudaStream_t st)
+{
+    CK(h, cudaEventRecord(h->ev_join, h->hs2));
+    CK(h, cudaStreamWaitEvent(st, h->ev_join, 0));
+    return STFWI_OK;
 }
 
 // record the whole forward pass (kind 0) or illumination pass (kind 2)
@@ -591,6 +637,9 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
     // with checkpoints the history is written later, segment by segment
     const bool hist = store && h->ncp == 0;
     if (hist) snap_state(h, st);
+    // the checkpoint copies take every shot: one chain then
+    const bool split = two_chains(h) && !(store && h->ncp > 0);
+    if (split && (rc = fork_chain(h, st))) return rc;
     for (int n = 0; n < h->g.nt; ++n) {
         if (store && h->ncp > 0 && n % h->ck == 0) {
             stfwi_status r = copy_ckpt(h, n / h->ck, true, st);
@@ -600,8 +649,14 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
         o.row0 = (hist && h->g.fs) ? h->row0 : nullptr;
         o.slot = n + 1;
         o.slot_row0 = n;
-        fwd_step(h, n, o, st);
+        if (split) {
+            fwd_step(h, n, o, st, 0);
+            fwd_step(h, n, o, h->hs2, 1);
+        } else {
+            fwd_step(h, n, o, st);
+        }
     }
+    if (split && (rc = join_chain(h, st))) return rc;
     CK(h, cudaGetLastError());
     return STFWI_OK;
 }
@@ -1153,8 +1208,11 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         return STFWI_ERR_OOM;
     }
     if (cudaStreamCreateWithFlags(&h->hs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->hs2, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         stfwi_destroy(h);
         return STFWI_ERR_CUDA;
     }
@@ -1193,7 +1251,10 @@ void stfwi_destroy(stfwi_handle *h)
         for (cudaEvent_t e : h->pev[k]) cudaEventDestroy(e);
     if (h->ev_in) cudaEventDestroy(h->ev_in);
     if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     if (h->hs) cudaStreamDestroy(h->hs);
+    if (h->hs2) cudaStreamDestroy(h->hs2);
     delete h;
 }
 
@@ -1397,7 +1458,7 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
         const int thr = 256;
         if (g.nrec > 0)
             k_inject_last<<<(g.nshot * g.nrec + thr - 1) / thr, thr, 0, s>>>(g, h->rx, h->rz, h->rec_adj, h->A);
-        auto adj = [&](int n, int seg0, int seg1) {
+        auto adj = [&](int n, int seg0, int seg1, cudaStream_t as, int part) {
             const int ping = (g.nt - 1 - n) & 1;
             AdjIn ai{};
             ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = n - seg0;
@@ -1411,9 +1472,9 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
             ao.acc = h->acc; ao.want_exact = ex; ao.want_img = im; ao.hist_tma = h->hist_tma ? 1 : 0;
             ao.src_a = sr ? src_dev : nullptr; ao.rec_adj = h->rec_adj; ao.ping = ping;
             switch (h->d.fd_order) {
-            case 2: launch_adj_step<2>(h, n, ai, ao, s); break;
-            case 4: launch_adj_step<4>(h, n, ai, ao, s); break;
-            default: launch_adj_step<8>(h, n, ai, ao, s); break;
+            case 2: launch_adj_step<2>(h, n, ai, ao, as, part); break;
+            case 4: launch_adj_step<4>(h, n, ai, ao, as, part); break;
+            default: launch_adj_step<8>(h, n, ai, ao, as, part); break;
             }
         };
         if ((ex || im) && h->ncp > 0) {
@@ -1440,10 +1501,17 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
                     o.slot_row0 = n - seg0;
                     fwd_step(h, n, o, s);
                 }
-                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0, seg1);
+                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0, seg1, s, -1);
             }
+        } else if (two_chains(h)) {
+            if ((r = fork_chain(h, s))) return r;
+            for (int n = g.nt - 1; n >= 0; --n) {
+                adj(n, 0, g.nt, s, 0);
+                adj(n, 0, g.nt, h->hs2, 1);
+            }
+            if ((r = join_chain(h, s))) return r;
         } else {
-            for (int n = g.nt - 1; n >= 0; --n) adj(n, 0, g.nt);
+            for (int n = g.nt - 1; n >= 0; --n) adj(n, 0, g.nt, s, -1);
         }
         if (ex || im)
             k_finalize<<<(unsigned)((g.nd + 255) / 256), 256, 0, s>>>(g, h->acc_used, h->accp, h->lr_used, h->acc, h->accLr, h->L2M,

@@ -171,6 +171,39 @@ def test_batch_of_shots_matches_single_shots():
     assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
 
 
+def test_two_chain_pass_equals_one_chain():
+    """With every kernel grouping the shots alike (shot_group 2: four groups
+    of the 8 shots) a pass runs as two independent chains over the groups on
+    two streams; with sampled kernel timing on it runs as one chain.  The
+    traces agree bit for bit (each shot's arithmetic is the same) and the
+    gradients to FP64 rounding (the order of the atomic FP64 sums)."""
+    vs, vp, rho = C.model()
+    nt, fd, fs = 90, 8, True
+    rx = np.arange(1, C.NX - 1, 3, dtype=np.int32)
+    rz = np.ones_like(rx)
+    sx = np.array([3, 7, 11, 15, 19, 23, 27, 30])
+    sz = np.array([2, 5, 3, 6, 2, 4, 3, 5])
+    types = ["force", "moment"] * 4
+    wav = (O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9).astype(np.float32)
+    obs = np.random.default_rng(6).standard_normal((8, nt, len(rx))).astype(np.float32) * 1e-9
+    out = []
+    for every in (0, 7):
+        S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2)
+        S.set_model(vs, vp, rho)
+        S.set_receivers(rx, rz)
+        S.set_shots(sx, sz, types, wav)
+        S.profile(every)
+        S.forward(store=True)
+        rec = S.records()
+        mis = S.misfit(obs, 1, 1.0)
+        g = S.gradient(exact=True, imaging=True)
+        out.append((rec, mis, g["exact"][0], g["exact"][1], g["imaging"][0]))
+        S.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1:], out[1][1:]):
+        assert _rel(a, b) < 1e-12, _rel(a, b)
+
+
 def test_checkpointed_gradient_equals_store_all():
     """Checkpoint every k steps + recompute gives the gradient of the
     every-step history (the recompute is deterministic), for an explicit k
