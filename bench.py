@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-every", type=int, default=20)
     p.add_argument("--no-autotune", action="store_true", help="keep the default shots per block")
+    p.add_argument("--chains", type=int, default=0,
+                   help="chains a pass may be split into (stfwi_set_chains; 0: the library's default)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-vs-plain time-to-Vs-error measurement (N = 1 only)")
     return p.parse_args()
@@ -283,6 +285,8 @@ def main():
     # (untimed set-up)
     schedule = None if args.no_autotune else S.autotune(steps=20)
     tile_rows = dict(zip(("fwd_vel,fwd_str,adj_a", "adj_b"), S.tile_rows()))
+    if args.chains:
+        S.set_chains(args.chains)
     mis_d = torch.zeros(ns, dtype=torch.float64, device="cuda")
     g_d = torch.zeros((1, 3, cfg["nz"], cfg["nx"]), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
@@ -416,11 +420,11 @@ def main():
     step_bytes = nt * sum(kb.values())
     roof["step_achieved"] = step_bytes / (ms_step * 1e-3) / 1e9
     roof["step_frac"] = roof["step_achieved"] / peak
-    # stencil launches: 2 per forward step and 2 per adjoint step, twice when
-    # the pass runs as two chains (every kernel with the same shots per block
-    # and at least two groups); plus set-up, misfit and finalize
+    # stencil launches: 2 per forward step and 2 per adjoint step, once per
+    # chain when the pass is split (every kernel with the same shots per
+    # block: at most one chain per shot group); plus set-up, misfit, finalize
     spg = set(schedule.values()) if schedule else set()
-    chains = 2 if len(spg) == 1 and -(-ns // spg.pop()) >= 2 else 1
+    chains = min(args.chains or 2, -(-ns // spg.pop())) if len(spg) == 1 else 1
     launches = 4 * nt * chains + 6
 
     cpu = None

@@ -190,6 +190,16 @@ stfwi_status stfwi_set_tile_rows(stfwi_handle *h, int32_t rows_a, int32_t rows_b
 /* rows_out [2]: the tile heights in use (rows_a, rows_b). */
 stfwi_status stfwi_tile_rows(const stfwi_handle *h, int32_t *rows_out);
 
+/* Chains a forward or adjoint pass may be split into (1-4, default 2; no
+ * counterpart in the reference).  The shots never interact, so when all
+ * four stencil kernels group the shots alike, a pass without checkpoint
+ * segments and without sampled timing is recorded as `chains` independent
+ * chains of launches over consecutive shot groups, on separate streams
+ * joined at its end; their launches overlap on the GPU.  Traces are the
+ * same bit for bit; the FP64 sums differ only in the order of their atomic
+ * additions. */
+stfwi_status stfwi_set_chains(stfwi_handle *h, int32_t chains);
+
 /* Residual preparation that allocates nothing (no counterpart in the
  * reference): the same misfit and adjoint sources as stfwi_misfit, without a
  * handle, for callers that cannot call cudaMalloc -- e.g. a custom call made

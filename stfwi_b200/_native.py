@@ -28,7 +28,7 @@ EXPORTS = (
     "stfwi_grid_shape", "stfwi_profile", "stfwi_kernel_times", "stfwi_misfit_noalloc",
     "stfwi_set_postprocess", "stfwi_preconditioner", "stfwi_project_velocity", "stfwi_autotune",
     "stfwi_forward_frames", "stfwi_adjoint_frames", "stfwi_imaging_condition", "stfwi_set_wait_limit",
-    "stfwi_set_tile_rows", "stfwi_tile_rows",
+    "stfwi_set_tile_rows", "stfwi_tile_rows", "stfwi_set_chains",
 )
 
 # full wavefield frames (bit set, in this order)
@@ -122,6 +122,7 @@ def load():
         L.stfwi_set_wait_limit.argtypes = [H, ct.c_int64]
         L.stfwi_set_tile_rows.argtypes = [H, i32, i32]
         L.stfwi_tile_rows.argtypes = [H, vp]
+        L.stfwi_set_chains.argtypes = [H, i32]
         L.stfwi_adjoint_frames.argtypes = [H, u32, vp, vp, vp]
         L.stfwi_imaging_condition.argtypes = [ct.POINTER(StfwiImagingDesc)] + [vp] * 10 + [vp, vp]
         sz, f32 = ct.c_size_t, ct.c_float

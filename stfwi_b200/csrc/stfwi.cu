@@ -24,6 +24,7 @@ using namespace stfwi;
 namespace {
 
 constexpr int MAX_SOS = 16;
+constexpr int MAX_CHAINS = 4;   // chains a pass may be split into (streams per handle)
 
 struct GraphKey {
     int kind;    // 0 forward, 1 adjoint, 2 illumination
@@ -110,8 +111,13 @@ struct stfwi_handle {
     bool stored = false;  // last forward kept its strain history
 
     cudaStream_t hs = nullptr;
-    cudaStream_t hs2 = nullptr;   // second chain of a pass split over the shot groups
-    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join = nullptr;
+    // a pass split into chains over the shot groups: the chains it may use
+    // (1-4, stfwi_set_chains), the chains of the pass being recorded, and
+    // the streams of chains 1.. (chain 0 runs on the pass's own stream)
+    int chains = 2, nchain_cur = 1;
+    cudaStream_t hsx[MAX_CHAINS - 1] = {};
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr;
+    cudaEvent_t ev_join[MAX_CHAINS - 1] = {};
     // sampled kernel timing: pev[k] holds (start, stop) pairs per sampled step
     int prof_every = 0;
     std::vector<cudaEvent_t> pev[4];
@@ -424,27 +430,34 @@ inline void prof_mark(stfwi_handle *h, int k, int n, int which, cudaStream_t st)
     else cudaEventRecord(h->pev[k][idx], st);
 }
 
-// the shot groups of kernel k that a launch covers: all of them (part < 0),
-// the first half (part 0) or the rest (part 1) -- the two chains of a split
-// pass; the Geo of the launch carries the first group
+// the shot groups of kernel k that a launch covers: all of them (part < 0)
+// or chain `part`'s share of the h->nchain_cur chains of a split pass
+// (consecutive groups); the Geo of the launch carries the first group
 Geo part_geo(const stfwi_handle *h, int k, int part, int *ngroups)
 {
     Geo g = h->g;
-    const int G = h->grp[k], GA = (G + 1) / 2;
-    g.goff = part == 1 ? GA : 0;
-    *ngroups = part < 0 ? G : part == 0 ? GA : G - GA;
+    const int G = h->grp[k], C = h->nchain_cur;
+    if (part < 0) {
+        *ngroups = G;
+        return g;
+    }
+    const int a = G * part / C, b = G * (part + 1) / C;
+    g.goff = a;
+    *ngroups = b - a;
     return g;
 }
 
-// a pass may run as two independent chains over the shot groups (the shots
-// never interact, the shared sums are atomic) when every stencil kernel
-// groups the shots the same way -- a chain's kernels then touch exactly its
-// own shots -- there are at least two groups, and no sampled timing is on
-bool two_chains(const stfwi_handle *h)
+// chains a pass may run as: independent chains over the shot groups (the
+// shots never interact, the shared sums are atomic) when every stencil
+// kernel groups the shots the same way -- a chain's kernels then touch
+// exactly its own shots -- and no sampled timing is on; at most one chain
+// per group
+int pass_chains(const stfwi_handle *h)
 {
     for (int k = 1; k < 4; ++k)
-        if (h->spgk[k] != h->spgk[0] || h->grp[k] != h->grp[0]) return false;
-    return h->grp[0] >= 2 && h->prof_every == 0 && h->hs2 != nullptr;
+        if (h->spgk[k] != h->spgk[0] || h->grp[k] != h->grp[0]) return 1;
+    if (h->prof_every != 0) return 1;
+    return std::max(1, std::min(h->chains, h->grp[0]));
 }
 
 template <int FD, int R>
@@ -604,20 +617,23 @@ void fwd_step(stfwi_handle *h, int n, const FwdOut &o, cudaStream_t st, int part
     }
 }
 
-// fork the handle's second stream off `st` / join it back (event edges of
-// the captured graph)
-stfwi_status fork_chain(stfwi_handle *h, cudaStream_t st)
+// fork the streams of chains 1 .. C-1 off `st` / join them back (event
+// edges of the captured graph); C = h->nchain_cur
+stfwi_status fork_chains(stfwi_handle *h, cudaStream_t st)
 {
     CK(h, cudaEventRecord(h->ev_fork, st));
-    CK(h, cudaStreamWaitEvent(h->hs2, h->ev_fork, 0));
+    for (int c = 1; c < h->nchain_cur; ++c) CK(h, cudaStreamWaitEvent(h->hsx[c - 1], h->ev_fork, 0));
     return STFWI_OK;
 }
-stfwi_status join_chain(stfwi_handle *h, cudaStream_t st)
+stfwi_status join_chains(stfwi_handle *h, cudaStream_t st)
 {
-    CK(h, cudaEventRecord(h->ev_join, h->hs2));
-    CK(h, cudaStreamWaitEvent(st, h->ev_join, 0));
+    for (int c = 1; c < h->nchain_cur; ++c) {
+        CK(h, cudaEventRecord(h->ev_join[c - 1], h->hsx[c - 1]));
+        CK(h, cudaStreamWaitEvent(st, h->ev_join[c - 1], 0));
+    }
     return STFWI_OK;
 }
+cudaStream_t chain_stream(const stfwi_handle *h, cudaStream_t st, int c) { return c == 0 ? st : h->hsx[c - 1]; }
 
 // record the whole forward pass (kind 0) or illumination pass (kind 2)
 stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStream_t st)
@@ -638,8 +654,9 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
     const bool hist = store && h->ncp == 0;
     if (hist) snap_state(h, st);
     // the checkpoint copies take every shot: one chain then
-    const bool split = two_chains(h) && !(store && h->ncp > 0);
-    if (split && (rc = fork_chain(h, st))) return rc;
+    h->nchain_cur = (store && h->ncp > 0) ? 1 : pass_chains(h);
+    const bool split = h->nchain_cur > 1;
+    if (split && (rc = fork_chains(h, st))) return rc;
     for (int n = 0; n < h->g.nt; ++n) {
         if (store && h->ncp > 0 && n % h->ck == 0) {
             stfwi_status r = copy_ckpt(h, n / h->ck, true, st);
@@ -650,13 +667,12 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
         o.slot = n + 1;
         o.slot_row0 = n;
         if (split) {
-            fwd_step(h, n, o, st, 0);
-            fwd_step(h, n, o, h->hs2, 1);
+            for (int c = 0; c < h->nchain_cur; ++c) fwd_step(h, n, o, chain_stream(h, st, c), c);
         } else {
             fwd_step(h, n, o, st);
         }
     }
-    if (split && (rc = join_chain(h, st))) return rc;
+    if (split && (rc = join_chains(h, st))) return rc;
     CK(h, cudaGetLastError());
     return STFWI_OK;
 }
@@ -1207,12 +1223,14 @@ stfwi_status stfwi_create(const stfwi_desc *d, stfwi_handle **out)
         stfwi_destroy(h);
         return STFWI_ERR_OOM;
     }
-    if (cudaStreamCreateWithFlags(&h->hs, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->hs2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    bool sok = cudaStreamCreateWithFlags(&h->hs, cudaStreamNonBlocking) == cudaSuccess &&
+               cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int c = 0; c < MAX_CHAINS - 1 && sok; ++c)
+        sok = cudaStreamCreateWithFlags(&h->hsx[c], cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&h->ev_join[c], cudaEventDisableTiming) == cudaSuccess;
+    if (!sok) {
         stfwi_destroy(h);
         return STFWI_ERR_CUDA;
     }
@@ -1252,9 +1270,11 @@ void stfwi_destroy(stfwi_handle *h)
     if (h->ev_in) cudaEventDestroy(h->ev_in);
     if (h->ev_out) cudaEventDestroy(h->ev_out);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
-    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    for (int c = 0; c < MAX_CHAINS - 1; ++c) {
+        if (h->ev_join[c]) cudaEventDestroy(h->ev_join[c]);
+        if (h->hsx[c]) cudaStreamDestroy(h->hsx[c]);
+    }
     if (h->hs) cudaStreamDestroy(h->hs);
-    if (h->hs2) cudaStreamDestroy(h->hs2);
     delete h;
 }
 
@@ -1503,13 +1523,11 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
                 }
                 for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0, seg1, s, -1);
             }
-        } else if (two_chains(h)) {
-            if ((r = fork_chain(h, s))) return r;
-            for (int n = g.nt - 1; n >= 0; --n) {
-                adj(n, 0, g.nt, s, 0);
-                adj(n, 0, g.nt, h->hs2, 1);
-            }
-            if ((r = join_chain(h, s))) return r;
+        } else if ((h->nchain_cur = pass_chains(h)) > 1) {
+            if ((r = fork_chains(h, s))) return r;
+            for (int n = g.nt - 1; n >= 0; --n)
+                for (int c = 0; c < h->nchain_cur; ++c) adj(n, 0, g.nt, chain_stream(h, s, c), c);
+            if ((r = join_chains(h, s))) return r;
         } else {
             for (int n = g.nt - 1; n >= 0; --n) adj(n, 0, g.nt, s, -1);
         }
@@ -1825,6 +1843,19 @@ stfwi_status stfwi_set_tile_rows(stfwi_handle *h, int32_t rows_a, int32_t rows_b
         return fail(h, STFWI_ERR_INVALID, "tile rows (%d, %d): use 8 or 16", rows_a, rows_b);
     // the state and a kept history do not depend on the tiling
     return set_tiling(h, rows_a / NWARP, rows_b / NWARP);
+}
+
+stfwi_status stfwi_set_chains(stfwi_handle *h, int32_t chains)
+{
+    if (!h) return STFWI_ERR_INVALID;
+    if (chains < 1 || chains > MAX_CHAINS)
+        return fail(h, STFWI_ERR_INVALID, "chains %d outside [1, %d]", chains, MAX_CHAINS);
+    if (chains != h->chains) {
+        CK(h, cudaStreamSynchronize(h->hs));
+        h->chains = chains;
+        drop_graphs(h);   // the split is part of the captured graphs
+    }
+    return STFWI_OK;
 }
 
 stfwi_status stfwi_tile_rows(const stfwi_handle *h, int32_t *rows_out)

@@ -308,6 +308,10 @@ class Solver:
         self._ok(self.lib.stfwi_tile_rows(self.h, out.ctypes.data), "tile_rows")
         return int(out[0]), int(out[1])
 
+    def set_chains(self, chains):
+        """Chains (1-4) a pass may be split into over the shot groups; see stfwi_set_chains."""
+        self._ok(self.lib.stfwi_set_chains(self.h, int(chains)), "set_chains")
+
     def set_tile_rows(self, rows_a, rows_b):
         """Tile heights (8 or 16 rows) of fwd_vel/fwd_str/adj_a and of adj_b."""
         self._ok(self.lib.stfwi_set_tile_rows(self.h, int(rows_a), int(rows_b)), "set_tile_rows")

@@ -171,12 +171,13 @@ def test_batch_of_shots_matches_single_shots():
     assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
 
 
-def test_two_chain_pass_equals_one_chain():
+def test_split_passes_equal_one_chain():
     """With every kernel grouping the shots alike (shot_group 2: four groups
-    of the 8 shots) a pass runs as two independent chains over the groups on
-    two streams; with sampled kernel timing on it runs as one chain.  The
-    traces agree bit for bit (each shot's arithmetic is the same) and the
-    gradients to FP64 rounding (the order of the atomic FP64 sums)."""
+    of the 8 shots) a pass runs as 2, 3 or 4 independent chains over the
+    groups on separate streams; with sampled kernel timing on, or one chain
+    set, it runs as one.  The traces agree bit for bit (each shot's
+    arithmetic is the same) and the gradients to FP64 rounding (the order of
+    the atomic FP64 sums)."""
     vs, vp, rho = C.model()
     nt, fd, fs = 90, 8, True
     rx = np.arange(1, C.NX - 1, 3, dtype=np.int32)
@@ -187,11 +188,12 @@ def test_two_chain_pass_equals_one_chain():
     wav = (O.ricker(np.arange(nt) * C.DT, C.FC, 1.5 / C.FC) * 1e9).astype(np.float32)
     obs = np.random.default_rng(6).standard_normal((8, nt, len(rx))).astype(np.float32) * 1e-9
     out = []
-    for every in (0, 7):
+    for every, chains in ((7, 2), (0, 2), (0, 3), (0, 4), (0, 1)):
         S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2)
         S.set_model(vs, vp, rho)
         S.set_receivers(rx, rz)
         S.set_shots(sx, sz, types, wav)
+        S.set_chains(chains)
         S.profile(every)
         S.forward(store=True)
         rec = S.records()
@@ -199,9 +201,15 @@ def test_two_chain_pass_equals_one_chain():
         g = S.gradient(exact=True, imaging=True)
         out.append((rec, mis, g["exact"][0], g["exact"][1], g["imaging"][0]))
         S.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    for a, b in zip(out[0][1:], out[1][1:]):
-        assert _rel(a, b) < 1e-12, _rel(a, b)
+    for k in range(1, len(out)):
+        assert np.array_equal(out[0][0], out[k][0]), k
+        for a, b in zip(out[0][1:], out[k][1:]):
+            assert _rel(a, b) < 1e-12, (k, _rel(a, b))
+    S = _solver(nt, len(rx), 8, fd, fs)
+    for bad in (0, 5, -1):
+        with pytest.raises(ValueError):
+            S.set_chains(bad)
+    S.close()
 
 
 def test_checkpointed_gradient_equals_store_all():
