@@ -653,14 +653,18 @@ stfwi_status enqueue_forward(stfwi_handle *h, uint32_t flags, int comp, cudaStre
     // with checkpoints the history is written later, segment by segment
     const bool hist = store && h->ncp == 0;
     if (hist) snap_state(h, st);
-    // the checkpoint copies take every shot: one chain then
-    h->nchain_cur = (store && h->ncp > 0) ? 1 : pass_chains(h);
+    h->nchain_cur = pass_chains(h);
     const bool split = h->nchain_cur > 1;
-    if (split && (rc = fork_chains(h, st))) return rc;
+    const bool ckpt = store && h->ncp > 0;
+    if (split && !ckpt && (rc = fork_chains(h, st))) return rc;
     for (int n = 0; n < h->g.nt; ++n) {
-        if (store && h->ncp > 0 && n % h->ck == 0) {
+        if (ckpt && n % h->ck == 0) {
+            // the checkpoint copy takes every shot: the chains join before
+            // it and fork again after it
+            if (split && n > 0 && (rc = join_chains(h, st))) return rc;
             stfwi_status r = copy_ckpt(h, n / h->ck, true, st);
             if (r) return r;
+            if (split && (rc = fork_chains(h, st))) return rc;
         }
         o.snap = hist ? h->snap : nullptr;
         o.row0 = (hist && h->g.fs) ? h->row0 : nullptr;
@@ -1516,12 +1520,25 @@ stfwi_status stfwi_gradient(stfwi_handle *h, uint32_t mode, double *g_out, float
                 FwdOut o{};
                 o.rec = h->rec; o.status = h->status; o.slots = h->slots;
                 o.snap = h->snap; o.row0 = g.fs ? h->row0 : nullptr;
+                // the segment's recompute and adjoint steps in chains over
+                // the shot groups; the copies above take every shot
+                const int C = h->nchain_cur = pass_chains(h);
+                if (C > 1 && (r = fork_chains(h, s))) return r;
                 for (int n = seg0; n < seg1; ++n) {
                     o.slot = n - seg0 + 1;
                     o.slot_row0 = n - seg0;
-                    fwd_step(h, n, o, s);
+                    if (C > 1)
+                        for (int q = 0; q < C; ++q) fwd_step(h, n, o, chain_stream(h, s, q), q);
+                    else
+                        fwd_step(h, n, o, s);
                 }
-                for (int n = seg1 - 1; n >= seg0; --n) adj(n, seg0, seg1, s, -1);
+                for (int n = seg1 - 1; n >= seg0; --n) {
+                    if (C > 1)
+                        for (int q = 0; q < C; ++q) adj(n, seg0, seg1, chain_stream(h, s, q), q);
+                    else
+                        adj(n, seg0, seg1, s, -1);
+                }
+                if (C > 1 && (r = join_chains(h, s))) return r;
             }
         } else if ((h->nchain_cur = pass_chains(h)) > 1) {
             if ((r = fork_chains(h, s))) return r;

@@ -171,11 +171,13 @@ def test_batch_of_shots_matches_single_shots():
     assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
 
 
-def test_split_passes_equal_one_chain():
+@pytest.mark.parametrize("ckpt", [0, 7])
+def test_split_passes_equal_one_chain(ckpt):
     """With every kernel grouping the shots alike (shot_group 2: four groups
     of the 8 shots) a pass runs as 2, 3 or 4 independent chains over the
     groups on separate streams; with sampled kernel timing on, or one chain
-    set, it runs as one.  The traces agree bit for bit (each shot's
+    set, it runs as one.  With checkpoints every 7 steps the chains join
+    around every checkpoint copy.  The traces agree bit for bit (each shot's
     arithmetic is the same) and the gradients to FP64 rounding (the order of
     the atomic FP64 sums)."""
     vs, vp, rho = C.model()
@@ -189,7 +191,7 @@ def test_split_passes_equal_one_chain():
     obs = np.random.default_rng(6).standard_normal((8, nt, len(rx))).astype(np.float32) * 1e-9
     out = []
     for every, chains in ((7, 2), (0, 2), (0, 3), (0, 4), (0, 1)):
-        S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2)
+        S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2, ckpt_interval=ckpt)
         S.set_model(vs, vp, rho)
         S.set_receivers(rx, rz)
         S.set_shots(sx, sz, types, wav)
