@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile-every", type=int, default=20)
     p.add_argument("--no-autotune", action="store_true", help="keep the default shots per block")
+    p.add_argument("--shot-group", type=int, default=0,
+                   help="shots per block of every kernel (0: autotuned)")
     p.add_argument("--chains", type=int, default=0,
                    help="chains a pass may be split into (stfwi_set_chains; 0: the library's default)")
     p.add_argument("--no-learned", action="store_true",
@@ -268,7 +270,7 @@ def main():
     wav = Mo.ricker(np.arange(nt) * cfg["dt"], cfg["fc"], 1.5 / cfg["fc"]).astype(np.float32)
     S = Solver(cfg["nz"], cfg["nx"], cfg["dx"], cfg["dz"], cfg["dt"], nt, cfg["fc"], cfg["pad"],
                len(rx), ns, fd_order=cfg["fd_order"], free_surface=cfg["free_surface"],
-               want_gradient=True)
+               want_gradient=True, shot_group=args.shot_group)
     S.set_receivers(rx, rz)
     S.set_shots(sx, sz, types, wav)
     comp = 1

@@ -1843,8 +1843,12 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
     const double sa[2] = {best[0][0] + best[0][1] + best[0][2], best[1][0] + best[1][1] + best[1][2]};
     const int qa = sa[0] < sa[1] ? 0 : 1, qb = best[0][3] < best[1][3] ? 0 : 1;
     if ((r = set_tiling(h, qa + 1, qb + 1))) return r;
-    const int spg[4] = {pick[qa][0], pick[qa][1], pick[qa][2], pick[qb][3]};
+    int spg[4] = {pick[qa][0], pick[qa][1], pick[qa][2], pick[qb][3]};
     for (int k = 0; k < 4; ++k) h->tuned[k] = spg[k];
+    // a descriptor shot_group > 0 keeps its shots per block (the tile
+    // shapes are still the tuned ones)
+    if (h->d.shot_group > 0)
+        for (int k = 0; k < 4; ++k) spg[k] = h->d.shot_group;
     set_groups(h, spg);
     drop_graphs(h);
     h->stored = false;   // the timing passes overwrote the state

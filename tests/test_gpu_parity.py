@@ -433,6 +433,13 @@ def test_autotuned_schedule_gives_the_same_gradient():
         S.close()
     for a, b in zip(res[1], res[0]):
         assert _rel(a, b) < 1e-6, _rel(a, b)
+    # a descriptor shot_group keeps its shots per block; the tile shapes are tuned
+    S = _solver(nt, len(rx), 7, fd, fs, want_gradient=True, shot_group=2)
+    S.set_model(vs, vp, rho)
+    S.set_receivers(rx, rz)
+    S.set_shots(sx, sz, types, wav)
+    assert set(S.autotune(steps=6).values()) == {2}
+    S.close()
 
 
 def test_config1_single_shot_gradient_vs_oracle():
