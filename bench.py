@@ -422,6 +422,9 @@ def main():
     step_bytes = nt * sum(kb.values())
     roof["step_achieved"] = step_bytes / (ms_step * 1e-3) / 1e9
     roof["step_frac"] = roof["step_achieved"] / peak
+    # for context: the nominal HBM3e bandwidth of an HGX B200 (7.7 TB/s)
+    roof["frac_of_nominal_7700"] = achieved / 7700.0
+    roof["step_frac_of_nominal_7700"] = roof["step_achieved"] / 7700.0
     # stencil launches: 2 per forward step and 2 per adjoint step, once per
     # chain when the pass is split (every kernel with the same shots per
     # block: at most one chain per shot group); plus set-up, misfit, finalize
