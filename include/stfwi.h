@@ -178,9 +178,11 @@ stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out);
  * lists), one for adj_b, and the shots per block of each of the four
  * stencil kernels (also across later stfwi_set_shots calls); spg_out [4]
  * (optional) receives the shots per block of fwd_vel, fwd_str, adj_a, adj_b,
- * stfwi_tile_rows the tile shapes.  Overwrites the fields and history: call
- * it before the forward whose history a gradient will use.  A descriptor
- * shot_group > 0 overrides the shots per block. */
+ * stfwi_tile_rows the tile shapes.  A second stage times whole steps split
+ * into chains as the passes will be (stfwi_set_chains) for those picks and
+ * for each uniform grouping, and keeps the fastest.  Overwrites the fields
+ * and history: call it before the forward whose history a gradient will
+ * use.  A descriptor shot_group > 0 overrides the shots per block. */
 stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, void *stream);
 
 /* Tile heights in rows (8 or 16; 16 and 16 until the autotuner has run):

@@ -1757,6 +1757,44 @@ stfwi_status stfwi_kernel_times(stfwi_handle *h, double *out)
     return STFWI_OK;
 }
 
+// `steps` forward then `steps` adjoint steps of the handle's current
+// schedule, launched directly (not captured) on `st`, split into chains
+// exactly as a captured pass would be (pass_chains); the timing passes of
+// the autotuner
+static stfwi_status enqueue_timing_steps(stfwi_handle *h, int steps, cudaStream_t st)
+{
+    const Geo &g = h->g;
+    stfwi_status r;
+    if ((r = zero_forward_state(h, st)) || (r = zero_adjoint_state(h, st))) return r;
+    const int C = h->nchain_cur = pass_chains(h);
+    if (C > 1 && (r = fork_chains(h, st))) return r;
+    FwdOut o{};
+    o.rec = h->rec; o.status = h->status; o.slots = h->slots;
+    for (int n = 0; n < steps; ++n)
+        for (int q = 0; q < C; ++q) fwd_step(h, n, o, chain_stream(h, st, q), C > 1 ? q : -1);
+    const bool ex = h->snap != nullptr;
+    for (int n = steps - 1; n >= 0; --n) {
+        AdjIn ai{};
+        ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = 0;
+        ai.accLr = h->accLr; ai.want_exact = ex && g.fs; ai.ping = n & 1;
+        AdjOut ao{};
+        ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = 0; ao.slot_img = h->slots > 1 ? 1 : -1;
+        ao.slot_next = -1; ao.accp = h->accp; ao.acc = h->acc; ao.want_exact = ex; ao.want_img = 0;
+        ao.rec_adj = h->rec_adj; ao.ping = n & 1; ao.hist_tma = h->hist_tma ? 1 : 0;
+        for (int q = 0; q < C; ++q) {
+            cudaStream_t cs = chain_stream(h, st, q);
+            const int part = C > 1 ? q : -1;
+            switch (h->d.fd_order) {
+            case 2: launch_adj_step<2>(h, n, ai, ao, cs, part); break;
+            case 4: launch_adj_step<4>(h, n, ai, ao, cs, part); break;
+            default: launch_adj_step<8>(h, n, ai, ao, cs, part); break;
+            }
+        }
+    }
+    if (C > 1 && (r = join_chains(h, st))) return r;
+    return STFWI_OK;
+}
+
 stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, void *stream)
 {
     stfwi_status rc = ready(h);
@@ -1792,25 +1830,8 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
         if (c > h->nshot) break;
         const int spg[4] = {c, c, c, c};
         set_groups(h, spg);
-        if ((r = zero_forward_state(h, st)) || (r = zero_adjoint_state(h, st))) break;
-        FwdOut o{};
-        o.rec = h->rec; o.status = h->status; o.slots = h->slots;
-        for (int n = 0; n < steps; ++n) fwd_step(h, n, o, st);
-        const bool ex = h->snap != nullptr;
-        for (int n = steps - 1; n >= 0; --n) {
-            AdjIn ai{};
-            ai.rec_adj = h->rec_adj; ai.row0 = h->row0; ai.slots = h->slots; ai.slot = 0;
-            ai.accLr = h->accLr; ai.want_exact = ex && g.fs; ai.ping = n & 1;
-            AdjOut ao{};
-            ao.snap = h->snap; ao.slots = h->slots; ao.slot_in = 0; ao.slot_img = h->slots > 1 ? 1 : -1;
-            ao.slot_next = -1; ao.accp = h->accp; ao.acc = h->acc; ao.want_exact = ex; ao.want_img = 0;
-            ao.rec_adj = h->rec_adj; ao.ping = n & 1; ao.hist_tma = h->hist_tma ? 1 : 0;
-            switch (h->d.fd_order) {
-            case 2: launch_adj_step<2>(h, n, ai, ao, st); break;
-            case 4: launch_adj_step<4>(h, n, ai, ao, st); break;
-            default: launch_adj_step<8>(h, n, ai, ao, st); break;
-            }
-        }
+        // one chain here: the sampled timing (prof_every = 1) is on
+        if ((r = enqueue_timing_steps(h, steps, st))) break;
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) {
@@ -1844,6 +1865,52 @@ stfwi_status stfwi_autotune(stfwi_handle *h, int32_t steps, int32_t *spg_out, vo
     const int qa = sa[0] < sa[1] ? 0 : 1, qb = best[0][3] < best[1][3] ? 0 : 1;
     if ((r = set_tiling(h, qa + 1, qb + 1))) return r;
     int spg[4] = {pick[qa][0], pick[qa][1], pick[qa][2], pick[qb][3]};
+    // stage 2: whole steps, split into chains as the passes will be.  The
+    // per-kernel picks let a pass split only when they coincide; a uniform
+    // grouping always does.  Time the picks and every uniform grouping and
+    // keep the fastest.
+    if (h->d.shot_group <= 0 && h->chains > 1) {
+        // no sampled timing while timing whole steps (it would also keep
+        // the passes in one chain)
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CK(h, cudaEventCreate(&e0));
+        if (cudaEventCreate(&e1) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            return fail(h, STFWI_ERR_CUDA, "autotune: cudaEventCreate failed");
+        }
+        const int keep_every = h->prof_every;
+        h->prof_every = 0;
+        double best_ms = 1e300;
+        int keep[4] = {spg[0], spg[1], spg[2], spg[3]};
+        for (int ci = -1; ci < (int)(sizeof(cand) / sizeof(cand[0])) && !r; ++ci) {
+            int trial[4];
+            if (ci < 0) {
+                for (int k = 0; k < 4; ++k) trial[k] = spg[k];
+            } else {
+                if (cand[ci] > h->nshot) break;
+                for (int k = 0; k < 4; ++k) trial[k] = cand[ci];
+            }
+            set_groups(h, trial);
+            float ms = 0.f;
+            for (int rep = 0; rep < 2 && !r; ++rep) {   // the first run warms up
+                if (rep == 1 && cudaEventRecord(e0, st) != cudaSuccess) r = STFWI_ERR_CUDA;
+                if (!r) r = enqueue_timing_steps(h, steps, st);
+            }
+            if (!r && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                       cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                r = fail(h, STFWI_ERR_CUDA, "autotune: timing of whole steps failed");
+            if (!r && ms < best_ms) {
+                best_ms = ms;
+                for (int k = 0; k < 4; ++k) keep[k] = trial[k];
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaGetLastError();
+        h->prof_every = keep_every;
+        if (r) return r;
+        for (int k = 0; k < 4; ++k) spg[k] = keep[k];
+    }
     for (int k = 0; k < 4; ++k) h->tuned[k] = spg[k];
     // a descriptor shot_group > 0 keeps its shots per block (the tile
     // shapes are still the tuned ones)
