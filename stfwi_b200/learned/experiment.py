@@ -246,7 +246,7 @@ def evaluate_multiband(net, seeds, K=4, bands=BANDS, iters=20, geom=I.GEOMETRY, 
                        log=print):
     """Learned vs plain on held-out models over the multiscale schedule.
 
-    Plain (the fallback and the judge): for each band in turn, the misfit
+    Plain (the fallback and the yardstick): for each band in turn, the misfit
     filter is set to its cutoff, the illumination preconditioner is
     recomputed at the current Vs, and the reference's L-BFGS
     (``I.lbfgs_reference``: history 100, 5 % step cap, strong Wolfe line
