@@ -72,7 +72,6 @@ struct stfwi_handle {
     int grp[4] = {1, 1, 1, 1}, spgk[4] = {1, 1, 1, 1};
     int acc_groups = 1, acc_used = 1;
     int lr_used = 1;  // rows of accLr written by the U_a/V_a phase (one per block row of shots)
-    int occ[4] = {1, 1, 1, 1};  // resident blocks per SM of fwd_vel, fwd_str, adj_a, adj_b
     int tuned[4] = {0, 0, 0, 0};  // shots per block chosen by stfwi_autotune (0: default)
 
     // shots / receivers
@@ -764,13 +763,8 @@ stfwi_status set_smem(stfwi_handle *h, const void *const (&kern)[7])
 {
     const size_t bytes[] = {Lk::bytes(Lk::VEL, 2), Lk::bytes(Lk::STR, 2), Lk::bytes(Lk::ADA, 2), Lk::bytes(Lk::ADB, 2),
                             Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2), Lk::bytes(Lk::ADB, 2)};
-    for (int k = 0; k < 7; ++k) {
+    for (int k = 0; k < 7; ++k)
         CK(h, cudaFuncSetAttribute(kern[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[k]));
-        if (k < 4) {
-            CK(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&h->occ[k], kern[k], NTHR, bytes[k]));
-            h->occ[k] = std::max(1, h->occ[k]);
-        }
-    }
     return STFWI_OK;
 }
 

@@ -171,8 +171,8 @@ def test_batch_of_shots_matches_single_shots():
     assert _rel(g, gsum) < 1e-5, _rel(g, gsum)
 
 
-@pytest.mark.parametrize("ckpt", [0, 7])
-def test_split_passes_equal_one_chain(ckpt):
+@pytest.mark.parametrize("ckpt,density", [(0, False), (7, False), (0, True), (7, True)])
+def test_split_passes_equal_one_chain(ckpt, density):
     """With every kernel grouping the shots alike (shot_group 2: four groups
     of the 8 shots) a pass runs as 2, 3 or 4 independent chains over the
     groups on separate streams; with sampled kernel timing on, or one chain
@@ -191,7 +191,8 @@ def test_split_passes_equal_one_chain(ckpt):
     obs = np.random.default_rng(6).standard_normal((8, nt, len(rx))).astype(np.float32) * 1e-9
     out = []
     for every, chains in ((7, 2), (0, 2), (0, 3), (0, 4), (0, 1)):
-        S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2, ckpt_interval=ckpt)
+        S = _solver(nt, len(rx), 8, fd, fs, want_gradient=True, shot_group=2, ckpt_interval=ckpt,
+                    density=density)
         S.set_model(vs, vp, rho)
         S.set_receivers(rx, rz)
         S.set_shots(sx, sz, types, wav)
@@ -201,7 +202,8 @@ def test_split_passes_equal_one_chain(ckpt):
         rec = S.records()
         mis = S.misfit(obs, 1, 1.0)
         g = S.gradient(exact=True, imaging=True)
-        out.append((rec, mis, g["exact"][0], g["exact"][1], g["imaging"][0]))
+        out.append((rec, mis, g["exact"][0], g["exact"][1], g["imaging"][0])
+                   + ((g["exact"][2], g["imaging"][2]) if density else ()))
         S.close()
     for k in range(1, len(out)):
         assert np.array_equal(out[0][0], out[k][0]), k
